@@ -1,0 +1,342 @@
+"""analogsat_b200 -- B200-native (sm_100a) AnalogSAT CTDS SAT/MAXSAT solver.
+
+Python mirror of the reference library's problem/solver API over the C ABI in
+``include/analogsat_b200.h`` (the C++ mirror is ``include/analogsat_b200.hpp``):
+
+* :class:`SatProblem`  -- ``analogsat::SatProblem`` (+ ``CnfReader``/``CnfWriter``);
+* :class:`SatSolver`   -- ``analogsat::SatSolver`` for a batch of instances x
+  trajectories, run in one persistent CUDA launch;
+* :func:`get_derivatives` / :func:`clause_violation_counts` -- ``ISat``'s
+  ``GetDerivatives`` / ``GetClauseViolationCount`` over many device-resident states.
+
+Method names follow the reference (``SetMaxTime``, ``SetSatState``, ``Solve``,
+``GetStepCount`` ...); errors raise :class:`AnalogSatError`, the reference's
+exceptions' counterpart.  Every call goes to the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from enum import IntEnum
+
+import numpy as np
+
+from . import _abi
+from ._abi import AnalogSatError, AS_PREC_F32_LOGA, AS_PREC_F64, check, load
+
+__all__ = [
+    "SatResult", "SatProblem", "SatSolver", "AnalogSatError", "AS_PREC_F32_LOGA", "AS_PREC_F64",
+    "get_derivatives", "clause_violation_counts", "load", "sat_result_message",
+]
+
+
+class SatResult(IntEnum):
+    """AnalogSAT/solver/SatResult.h:24-32"""
+    SAT_SOLUTION_FOUND = 0
+    SAT_UNDERFLOW = 1
+    SAT_ODE_INTERRUPTED = 2
+    SAT_MAXTIME_REACHED = 3
+    SAT_MAXITER_REACHED = 4
+    SAT_UNKNOWN = 5
+
+
+_MESSAGES = {0: "solution found", 1: "underflow", 2: "user interrupt", 3: "maximum time reached",
+             4: "maximum steps reached"}
+
+
+def sat_result_message(r: int) -> str:
+    """GetSatResultMessage (AnalogSAT/solver/SatResult.cpp:21-33)."""
+    return _MESSAGES.get(int(r), "unknown result")
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a: np.ndarray, t=C.c_int32):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class SatProblem:
+    """A CNF formula (AnalogSAT/problem/SatProblem.h:26-63)."""
+
+    def __init__(self, handle=None):
+        self._lib = load()
+        self._h = handle
+
+    @classmethod
+    def from_arrays(cls, literals, lengths) -> "SatProblem":
+        """SatProblem::AddClauses(literals, lengths) (SatProblem.cpp:64-95)."""
+        lits, lens = _i32(literals), _i32(lengths)
+        if lens.size and lens.sum() != lits.size:
+            raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "lengths do not sum to the literal count")
+        h = C.c_void_p()
+        check(load().as_problem_create(_ptr(lits), _ptr(lens), int(lens.size), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_clauses(cls, clauses) -> "SatProblem":
+        """SatProblem::AddClauses(vector<vector<int>>) (SatProblem.cpp:97-103)."""
+        lens = [len(c) for c in clauses]
+        lits = [l for c in clauses for l in c]
+        return cls.from_arrays(lits, lens)
+
+    @classmethod
+    def read_cnf(cls, path: str) -> "SatProblem":
+        """CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141)."""
+        h = C.c_void_p()
+        msg = C.create_string_buffer(256)
+        check(load().as_problem_read_cnf(path.encode(), C.byref(h), msg, 256))
+        return cls(h)
+
+    def write_cnf(self, path: str) -> None:
+        """CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74)."""
+        check(self._lib.as_problem_write_cnf(self._h, path.encode()))
+
+    def _nmk(self):
+        n, m, k = C.c_int32(), C.c_int32(), C.c_int32()
+        check(self._lib.as_problem_get_nmk(self._h, C.byref(n), C.byref(m), C.byref(k)))
+        return n.value, m.value, k.value
+
+    def Get_N(self) -> int:
+        return self._nmk()[0]
+
+    def Get_M(self) -> int:
+        return self._nmk()[1]
+
+    def Get_K(self) -> int:
+        return self._nmk()[2]
+
+    @property
+    def n(self) -> int:
+        return self.Get_N()
+
+    @property
+    def m(self) -> int:
+        return self.Get_M()
+
+    @property
+    def k(self) -> int:
+        return self.Get_K()
+
+    def GetAllClauses(self):
+        """SatProblem::GetAllClauses (SatProblem.cpp:104-110) -> (literals, lengths)."""
+        nl = check(self._lib.as_problem_num_literals(self._h))
+        lits = np.zeros(max(nl, 1), np.int32)
+        lens = np.zeros(max(self.m, 1), np.int32)
+        check(self._lib.as_problem_get_clauses(self._h, _ptr(lits), _ptr(lens)))
+        return lits[:nl], lens[: self.m]
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.as_problem_free(self._h)
+        except Exception:
+            pass
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        try:
+            import torch
+            return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            return C.c_void_p(0)
+    return C.c_void_p(int(stream))
+
+
+def get_derivatives(problem: SatProblem, x, out=None, logspace: bool = False, stream=None):
+    """ISat::GetDerivatives for a [B, N+M] CUDA tensor of public states (float32 or
+    float64).  float64 follows CpuSat<double> bit for bit; float32 with logspace=True
+    treats the a-block as ln a and returns d(ln a)/dt = K^2."""
+    import torch
+    if not x.is_cuda:
+        raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "get_derivatives needs a CUDA tensor")
+    x = x.contiguous()
+    if out is None:
+        out = torch.empty_like(x)
+    B = x.shape[0] if x.dim() == 2 else 1
+    lib = load()
+    if x.dtype == torch.float64:
+        if logspace:
+            raise AnalogSatError(_abi.AS_ERR_UNSUPPORTED, "log-space RHS is FP32 only")
+        check(lib.as_rhs_f64(problem._h, C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()), B,
+                             _stream_ptr(stream)))
+    elif x.dtype == torch.float32:
+        check(lib.as_rhs_f32(problem._h, C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()), B,
+                             int(logspace), _stream_ptr(stream)))
+    else:
+        raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "x must be float32 or float64")
+    return out
+
+
+def clause_violation_counts(problem: SatProblem, x, stream=None):
+    """ISat::GetClauseViolationCount for a [B, N+M] CUDA tensor -> int32[B] (device)."""
+    import torch
+    x = x.contiguous()
+    B = x.shape[0] if x.dim() == 2 else 1
+    out = torch.empty(B, dtype=torch.int32, device=x.device)
+    lib = load()
+    fn = lib.as_violations_f64 if x.dtype == torch.float64 else lib.as_violations_f32
+    check(fn(problem._h, C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()), B,
+             _stream_ptr(stream)))
+    return out
+
+
+class SatSolver:
+    """Batched counterpart of ``SatSolver<TFloat,TState>`` (AnalogSAT/solver/SatSolver.h).
+
+    One solver holds several instances; ``SetSatStates`` assigns trajectories
+    (instance index + initial public state each) and ``Solve`` runs all of them to
+    their SatResult in one persistent launch.  Defaults are the reference's:
+    maxTime 100, maxSteps 1e5, batch 20, eps 1e-4.
+    """
+
+    def __init__(self, problems, precision: int = AS_PREC_F32_LOGA, device: int = -1):
+        if isinstance(problems, SatProblem):
+            problems = [problems]
+        self._lib = load()
+        self.problems = list(problems)
+        self.precision = precision
+        arr = (C.c_void_p * len(self.problems))(*[p._h for p in self.problems])
+        h = C.c_void_p()
+        check(self._lib.as_solver_create(arr, len(self.problems), precision, device, C.byref(h)))
+        self._h = h
+        self._nm = [(p.n, p.m) for p in self.problems]
+        self._traj_problem = None
+
+    # -- configuration (SatSolver.h:133-160, CpuRungeKutta.cpp:126-131) --
+    def SetMaxTime(self, v: float):
+        check(self._lib.as_solver_set_max_time(self._h, float(v)))
+
+    def SetMaxSteps(self, v: int):
+        check(self._lib.as_solver_set_max_steps(self._h, int(v)))
+
+    def SetBatchSize(self, v: int):
+        check(self._lib.as_solver_set_batch_size(self._h, int(v)))
+
+    def SetEpsilon(self, v: float):
+        check(self._lib.as_solver_set_epsilon(self._h, float(v)))
+
+    def SetWallBudget(self, seconds: float):
+        check(self._lib.as_solver_set_wall_budget(self._h, float(seconds)))
+
+    def SetStopOnFirst(self, flag: bool):
+        check(self._lib.as_solver_set_stop_on_first(self._h, int(bool(flag))))
+
+    def SetTrackBest(self, flag: bool):
+        check(self._lib.as_solver_set_track_best(self._h, int(bool(flag))))
+
+    def ForceThreads(self, threads: int):
+        check(self._lib.as_solver_force_threads(self._h, int(threads)))
+
+    # -- states (SatSolver::SetSatState, SatSolver.h:183-192) --
+    def SetSatStates(self, problem_index, states, stream=None):
+        """states: host array of the concatenated public vectors, or a CUDA tensor
+        (copied device-to-device on `stream`, default the current torch stream)."""
+        pi = _i32(problem_index)
+        self._traj_problem = pi.copy()
+        try:
+            import torch
+            is_tensor = isinstance(states, torch.Tensor)
+        except ImportError:
+            is_tensor = False
+        if is_tensor and states.is_cuda:
+            check(self._lib.as_solver_set_states_device(
+                self._h, _ptr(pi), int(pi.size), C.c_void_p(states.data_ptr()),
+                _stream_ptr(stream)))
+            return
+        if is_tensor:
+            states = states.numpy()
+        st = np.ascontiguousarray(states)
+        if st.dtype == np.float32:
+            check(self._lib.as_solver_set_states_f32(self._h, _ptr(pi), int(pi.size),
+                                                     st.ctypes.data_as(C.c_void_p)))
+        else:
+            st = np.ascontiguousarray(st, np.float64)
+            check(self._lib.as_solver_set_states_f64(self._h, _ptr(pi), int(pi.size),
+                                                     st.ctypes.data_as(C.c_void_p)))
+
+    def SetSatState(self, state, problem: int = 0):
+        """Single-trajectory form of SatSolver::SetSatState(vector)."""
+        self.SetSatStates([problem], np.asarray(state))
+
+    def Solve(self):
+        """SatSolver::Solve for every trajectory; returns the SatResult array."""
+        check(self._lib.as_solver_solve(self._h))
+        return self.results()["status"]
+
+    def SolveAsync(self, stream=None):
+        check(self._lib.as_solver_solve_async(self._h, _stream_ptr(stream) if stream else None))
+
+    def Sync(self):
+        check(self._lib.as_solver_sync(self._h))
+
+    def results(self) -> dict:
+        n = len(self._traj_problem)
+        st = np.zeros(n, np.int32); tm = np.zeros(n); sp = np.zeros(n, np.int32)
+        rh = np.zeros(n, np.int32); at = np.zeros(n, np.int32); vi = np.zeros(n, np.int32)
+        mv = np.zeros(n, np.int32); hd = np.zeros(n)
+        check(self._lib.as_solver_get_results(
+            self._h, _ptr(st), _ptr(tm, C.c_double), _ptr(sp), _ptr(rh), _ptr(at), _ptr(vi),
+            _ptr(mv), _ptr(hd, C.c_double)))
+        return dict(status=st, time=tm, steps=sp, rhs=rh, attempts=at, violations=vi,
+                    min_violations=mv, last_step=hd)
+
+    def GetSatStates(self, dtype=np.float64, out=None) -> np.ndarray:
+        """Final public states, concatenated (SatSolver::GetSatState().CopyTo).
+        `out` may be a preallocated (e.g. pinned) host array of the right size/dtype."""
+        total = int(sum(sum(self._nm[p]) for p in self._traj_problem))
+        if out is None:
+            out = np.zeros(total, dtype)
+        dtype = out.dtype
+        if out.size != total or not out.flags.c_contiguous:
+            raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "out has the wrong size or layout")
+        fn = (self._lib.as_solver_get_states_f32 if dtype == np.float32
+              else self._lib.as_solver_get_states_f64)
+        check(fn(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def GetSatState(self, traj: int = 0, dtype=np.float64) -> np.ndarray:
+        allst = self.GetSatStates(dtype)
+        off = int(sum(sum(self._nm[p]) for p in self._traj_problem[:traj]))
+        n, m = self._nm[self._traj_problem[traj]]
+        return allst[off: off + n + m]
+
+    def GetBestAssignment(self, traj: int) -> np.ndarray:
+        n, _ = self._nm[self._traj_problem[traj]]
+        bits = np.zeros((n + 31) // 32, np.uint32)
+        check(self._lib.as_solver_get_best_assignment(self._h, int(traj),
+                                                      bits.ctypes.data_as(C.c_void_p)))
+        return ((bits[np.arange(n) // 32] >> (np.arange(n) % 32).astype(np.uint32)) & 1).astype(bool)
+
+    def launch_shape(self) -> dict:
+        a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        check(self._lib.as_solver_get_launch_shape(self._h, C.byref(a), C.byref(b), C.byref(c),
+                                                   C.byref(d)))
+        return dict(threads=a.value, ctas=b.value, smem_bytes=c.value, ctas_per_sm=d.value)
+
+    def states_device_ptr(self) -> int:
+        return int(self._lib.as_solver_states_device(self._h) or 0)
+
+    # single-trajectory getters (SatSolver.h:77-130) for trajectory 0
+    def GetStepCount(self, traj: int = 0) -> int:
+        return int(self.results()["steps"][traj])
+
+    def GetRhsCount(self, traj: int = 0) -> int:
+        return int(self.results()["rhs"][traj])
+
+    def GetElapsedTime(self, traj: int = 0) -> float:
+        return float(self.results()["time"][traj])
+
+    def GetLastStepSize(self, traj: int = 0) -> float:
+        return float(self.results()["last_step"][traj])
+
+    def GetLastClauseViolationCount(self, traj: int = 0) -> int:
+        return int(self.results()["violations"][traj])
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.as_solver_free(self._h)
+        except Exception:
+            pass

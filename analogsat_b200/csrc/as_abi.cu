@@ -1,0 +1,783 @@
+// C ABI of the AnalogSAT B200 solver (declarations and reference mapping in
+// include/analogsat_b200.h).  Host logic: problem handles, device packing,
+// launch-shape selection, the persistent solve launch (captured in a CUDA graph),
+// and the batched RHS / clause-check primitives.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/analogsat_b200.h"
+#include "as_kernels.cuh"
+#include "as_problem.h"
+
+using namespace asb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define AS_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(AS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t b) {
+        if (b <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(b, 16));
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Device copy of one or more packed instances in a single pool.
+struct DevicePool {
+    int device = -1;
+    DevBuf lit, sell_row, sell, inst;
+    std::vector<DevInstance> host_inst;
+
+    int upload(const std::vector<const PackedProblem*>& pk, int dev) {
+        size_t nl = 0, nr = 0, ns = 0;
+        for (auto* q : pk) {
+            nl += q->lit.size();
+            nr += q->sell_row.size();
+            ns += q->sell.size();
+        }
+        AS_CUDA(lit.alloc(std::max<size_t>(nl, 1) * 4));
+        AS_CUDA(sell_row.alloc(std::max<size_t>(nr, 1) * 4));
+        AS_CUDA(sell.alloc(std::max<size_t>(ns, 1) * 4));
+        AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
+        host_inst.clear();
+        size_t ol = 0, orr = 0, os = 0;
+        for (auto* q : pk) {
+            DevInstance d;
+            d.n = q->n; d.m = q->m; d.k = q->k; d.mp = q->mp; d.nslices = q->nslices; d.pad = 0;
+            d.lit = lit.as<uint32_t>() + ol;
+            d.sell_row = sell_row.as<int32_t>() + orr;
+            d.sell = sell.as<int32_t>() + os;
+            if (!q->lit.empty())
+                AS_CUDA(cudaMemcpy((void*)d.lit, q->lit.data(), q->lit.size() * 4, cudaMemcpyHostToDevice));
+            if (!q->sell_row.empty())
+                AS_CUDA(cudaMemcpy((void*)d.sell_row, q->sell_row.data(), q->sell_row.size() * 4,
+                                   cudaMemcpyHostToDevice));
+            if (!q->sell.empty())
+                AS_CUDA(cudaMemcpy((void*)d.sell, q->sell.data(), q->sell.size() * 4, cudaMemcpyHostToDevice));
+            ol += q->lit.size();
+            orr += q->sell_row.size();
+            os += q->sell.size();
+            host_inst.push_back(d);
+        }
+        AS_CUDA(cudaMemcpy(inst.p, host_inst.data(), sizeof(DevInstance) * host_inst.size(),
+                           cudaMemcpyHostToDevice));
+        device = dev;
+        return AS_OK;
+    }
+};
+
+int current_device(int requested, int* out) {
+    if (requested >= 0) {
+        AS_CUDA(cudaSetDevice(requested));
+        *out = requested;
+        return AS_OK;
+    }
+    AS_CUDA(cudaGetDevice(out));
+    return AS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// compiled launch shapes of the persistent solver
+// ---------------------------------------------------------------------------
+using SolveFn = void (*)(SolveParams);
+
+struct Variant {
+    int precision;  // AS_PREC_*
+    int kmax, bt;
+    SolveFn fn;
+    size_t bytes_per_value;
+};
+
+#define AS_VARIANT_F32(K, BT) Variant{AS_PREC_F32_LOGA, K, BT, &solve_kernel<float, true, K, BT>, 4}
+#define AS_VARIANT_F64(K, BT) Variant{AS_PREC_F64, K, BT, &solve_kernel<double, false, K, BT>, 8}
+
+const std::vector<Variant>& variants() {
+    static const std::vector<Variant> v = {
+        AS_VARIANT_F32(3, 128),  AS_VARIANT_F32(3, 256),  AS_VARIANT_F32(3, 512),
+        AS_VARIANT_F32(3, 1024), AS_VARIANT_F32(4, 128),  AS_VARIANT_F32(4, 256),
+        AS_VARIANT_F32(4, 512),  AS_VARIANT_F32(4, 1024), AS_VARIANT_F32(16, 256),
+        AS_VARIANT_F32(16, 1024), AS_VARIANT_F64(3, 128), AS_VARIANT_F64(3, 256),
+        AS_VARIANT_F64(3, 512),  AS_VARIANT_F64(16, 256),
+    };
+    return v;
+}
+
+size_t solver_smem(const Variant& v, const PackedProblem& q) {
+    return solve_smem_values<float>(q.n, q.m, q.k, q.mp) * v.bytes_per_value;
+}
+
+bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_limit) {
+    return v.precision == precision && q.k <= v.kmax && solver_smem(v, q) <= smem_limit;
+}
+
+// Default CTA size: about four clauses per thread, 128..1024 threads.
+int preferred_bt(const PackedProblem& q) {
+    int bt = 128;
+    while (bt < 1024 && bt * 4 < q.m) bt *= 2;
+    return bt;
+}
+
+__global__ void stamp_deadline_kernel(unsigned long long* out, unsigned long long budget_ns) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *out = t + budget_ns;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// handles
+// ---------------------------------------------------------------------------
+struct as_problem {
+    HostProblem host;
+    PackedProblem packed;
+    DevicePool dev;  // lazily uploaded for the device primitives
+};
+
+struct as_solver {
+    int device = 0;
+    int precision = AS_PREC_F32_LOGA;
+    std::vector<PackedProblem> problems;
+    DevicePool pool;
+    int sm_count = 0;
+    size_t smem_limit = 0;
+
+    // SatSolver defaults (SatSolver.h:60-62) and CpuRungeKutta's eps (CpuRungeKutta.cpp:43)
+    double max_time = 100.0;
+    int max_steps = 100000;
+    int batch = 20;
+    double eps = 1e-4;
+    double wall_budget = 0.0;
+    int stop_on_first = 0;
+    int track_best = 0;
+    int forced_bt = 0;
+
+    // trajectories
+    int num_traj = 0;
+    std::vector<int> traj_problem;     // user order
+    std::vector<long long> traj_off;   // element offset of each trajectory (user order)
+    std::vector<long long> traj_bits;  // word offset into best_bits
+    long long total_values = 0;
+    std::vector<int> order;            // launch order -> user trajectory
+    struct Group { int variant, u0, u1; };
+    std::vector<Group> groups;
+
+    DevBuf states, results, unit_inst, unit_state, unit_bits, queue, solved, deadline, best_bits;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool graph_valid = false;
+    bool groups_dirty = true;
+    int last_bt = 0, last_ctas = 0, last_smem = 0, last_occ = 0;
+
+    ~as_solver() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void invalidate() { graph_valid = false; }
+};
+
+// Definitions below take C linkage from their declarations in analogsat_b200.h.
+
+int32_t as_last_error(char* buf, int32_t buf_len) {
+    if (buf && buf_len > 0) {
+        std::strncpy(buf, g_last_error.c_str(), buf_len - 1);
+        buf[buf_len - 1] = 0;
+    }
+    return (int32_t)g_last_error.size();
+}
+
+int32_t as_device_sm_count(int32_t device) {
+    int dev = 0, n = 0;
+    int r = current_device(device, &dev);
+    if (r) return r;
+    AS_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n;
+}
+
+// ---- problems ----
+int32_t as_problem_create(const int32_t* literals, const int32_t* lengths, int32_t num_clauses,
+                          as_problem** out) {
+    if (!out || num_clauses < 0 || (num_clauses > 0 && (!literals || !lengths)))
+        return fail(AS_ERR_BAD_INPUT, "as_problem_create: null argument or negative clause count");
+    for (int j = 0; j < num_clauses; j++)
+        if (lengths[j] < 0) return fail(AS_ERR_BAD_INPUT, "as_problem_create: negative clause length");
+    auto* p = new as_problem();
+    p->host.add_clauses(literals, lengths, num_clauses);
+    p->packed = pack(p->host);
+    *out = p;
+    return AS_OK;
+}
+
+int32_t as_problem_read_cnf(const char* path, as_problem** out, char* msg, int32_t msg_len) {
+    if (!path || !out) return fail(AS_ERR_BAD_INPUT, "as_problem_read_cnf: null argument");
+    auto* p = new as_problem();
+    std::string m;
+    bool ok = read_cnf(path, p->host, m);
+    if (msg && msg_len > 0) {
+        std::strncpy(msg, m.c_str(), msg_len - 1);
+        msg[msg_len - 1] = 0;
+    }
+    if (!ok) {
+        delete p;
+        return fail(AS_ERR_IO, "as_problem_read_cnf: " + m);
+    }
+    p->packed = pack(p->host);
+    *out = p;
+    return AS_OK;
+}
+
+int32_t as_problem_write_cnf(const as_problem* p, const char* path) {
+    if (!p || !path) return fail(AS_ERR_BAD_INPUT, "as_problem_write_cnf: null argument");
+    return write_cnf(path, p->host) ? AS_OK : fail(AS_ERR_IO, "as_problem_write_cnf: file open failed");
+}
+
+int32_t as_problem_get_nmk(const as_problem* p, int32_t* n, int32_t* m, int32_t* k) {
+    if (!p) return fail(AS_ERR_BAD_INPUT, "as_problem_get_nmk: null problem");
+    if (n) *n = p->host.n;
+    if (m) *m = p->host.m;
+    if (k) *k = p->host.k;
+    return AS_OK;
+}
+
+int32_t as_problem_num_literals(const as_problem* p) {
+    if (!p) return fail(AS_ERR_BAD_INPUT, "as_problem_num_literals: null problem");
+    return (int32_t)p->host.storage.size();
+}
+
+int32_t as_problem_get_clauses(const as_problem* p, int32_t* literals, int32_t* lengths) {
+    if (!p || !literals || !lengths) return fail(AS_ERR_BAD_INPUT, "as_problem_get_clauses: null argument");
+    size_t o = 0;
+    for (int j = 0; j < p->host.m; j++) {
+        lengths[j] = p->host.length[j];
+        for (int i = 0; i < p->host.length[j]; i++) literals[o++] = p->host.storage[p->host.start[j] + i];
+    }
+    return AS_OK;
+}
+
+void as_problem_free(as_problem* p) { delete p; }
+
+// ---- device primitives ----
+namespace {
+
+int ensure_uploaded(as_problem* p) {
+    if (p->host.m == 0 || p->host.k == 0) return fail(AS_ERR_NO_PROBLEM, "SAT problem has not been set");
+    int dev = 0;
+    AS_CUDA(cudaGetDevice(&dev));
+    if (p->dev.device == dev) return AS_OK;
+    std::vector<const PackedProblem*> v{&p->packed};
+    return p->dev.upload(v, dev);
+}
+
+template <typename T, bool LOGA, int KMAX>
+int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
+    constexpr int BT = 512;
+    const auto& q = p->packed;
+    const size_t smem = ((size_t)((q.n + 1 + 3) & ~3) + (size_t)q.k * q.mp) * sizeof(T);
+    auto fn = &rhs_batch_kernel<T, LOGA, KMAX, BT>;
+    int dev = 0, sms = 0, optin = 0, occ = 0;
+    AS_CUDA(cudaGetDevice(&dev));
+    AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > (size_t)optin)
+        return fail(AS_ERR_UNSUPPORTED, "instance too large for the shared-memory RHS kernel");
+    AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
+    const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
+    fn<<<grid, BT, smem, st>>>(p->dev.host_inst[0], x, d, ns, (long long)(q.n + q.m));
+    AS_CUDA(cudaGetLastError());
+    return AS_OK;
+}
+
+template <typename T, bool LOGA>
+int dispatch_rhs(as_problem* p, const T* x, T* d, int ns, void* stream) {
+    if (!p || !x || !d || ns < 0) return fail(AS_ERR_BAD_INPUT, "as_rhs: null argument");
+    if (ns == 0) return AS_OK;
+    int r = ensure_uploaded(p);
+    if (r) return r;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int k = p->packed.k;
+    if (k <= 3) return launch_rhs<T, LOGA, 3>(p, x, d, ns, st);
+    if (k <= 4) return launch_rhs<T, LOGA, 4>(p, x, d, ns, st);
+    if (k <= 16) return launch_rhs<T, LOGA, 16>(p, x, d, ns, st);
+    return fail(AS_ERR_UNSUPPORTED, "clause length > 16 is not supported");
+}
+
+template <typename T, int KMAX>
+int launch_viol(as_problem* p, const T* x, int* c, int ns, cudaStream_t st) {
+    constexpr int BT = 256;
+    const auto& q = p->packed;
+    const size_t smem = (size_t)((q.n + 1 + 3) & ~3) * sizeof(T);
+    auto fn = &viol_batch_kernel<T, KMAX, BT>;
+    int dev = 0, sms = 0, optin = 0, occ = 0;
+    AS_CUDA(cudaGetDevice(&dev));
+    AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > (size_t)optin) return fail(AS_ERR_UNSUPPORTED, "instance too large for the clause-check kernel");
+    AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
+    const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
+    fn<<<grid, BT, smem, st>>>(p->dev.host_inst[0], x, c, ns, (long long)(q.n + q.m));
+    AS_CUDA(cudaGetLastError());
+    return AS_OK;
+}
+
+template <typename T>
+int dispatch_viol(as_problem* p, const T* x, int* c, int ns, void* stream) {
+    if (!p || !x || !c || ns < 0) return fail(AS_ERR_BAD_INPUT, "as_violations: null argument");
+    if (ns == 0) return AS_OK;
+    int r = ensure_uploaded(p);
+    if (r) return r;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int k = p->packed.k;
+    if (k <= 3) return launch_viol<T, 3>(p, x, c, ns, st);
+    if (k <= 4) return launch_viol<T, 4>(p, x, c, ns, st);
+    if (k <= 16) return launch_viol<T, 16>(p, x, c, ns, st);
+    return fail(AS_ERR_UNSUPPORTED, "clause length > 16 is not supported");
+}
+
+}  // namespace
+
+int32_t as_rhs_f32(as_problem* p, const float* x, float* dxdt, int32_t num_states, int32_t logspace,
+                   void* stream) {
+    return logspace ? dispatch_rhs<float, true>(p, x, dxdt, num_states, stream)
+                    : dispatch_rhs<float, false>(p, x, dxdt, num_states, stream);
+}
+
+int32_t as_rhs_f64(as_problem* p, const double* x, double* dxdt, int32_t num_states, void* stream) {
+    return dispatch_rhs<double, false>(p, x, dxdt, num_states, stream);
+}
+
+int32_t as_violations_f32(as_problem* p, const float* x, int32_t* counts, int32_t num_states,
+                          void* stream) {
+    return dispatch_viol<float>(p, x, counts, num_states, stream);
+}
+
+int32_t as_violations_f64(as_problem* p, const double* x, int32_t* counts, int32_t num_states,
+                          void* stream) {
+    return dispatch_viol<double>(p, x, counts, num_states, stream);
+}
+
+// ---- solver ----
+int32_t as_solver_create(const as_problem* const* problems, int32_t num_problems, int32_t precision,
+                         int32_t device, as_solver** out) {
+    if (!out || !problems || num_problems <= 0)
+        return fail(AS_ERR_BAD_INPUT, "as_solver_create: need at least one problem");
+    if (precision != AS_PREC_F32_LOGA && precision != AS_PREC_F64)
+        return fail(AS_ERR_BAD_INPUT, "as_solver_create: unknown precision");
+    for (int i = 0; i < num_problems; i++) {
+        if (!problems[i]) return fail(AS_ERR_BAD_INPUT, "as_solver_create: null problem");
+        if (problems[i]->host.k == 0) return fail(AS_ERR_NO_PROBLEM, "SAT problem has not been set");
+    }
+    std::unique_ptr<as_solver> s(new as_solver());
+    int r = current_device(device, &s->device);
+    if (r) return r;
+    s->precision = precision;
+    for (int i = 0; i < num_problems; i++) s->problems.push_back(problems[i]->packed);
+    std::vector<const PackedProblem*> pk;
+    for (auto& q : s->problems) pk.push_back(&q);
+    r = s->pool.upload(pk, s->device);
+    if (r) return r;
+    int optin = 0;
+    AS_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
+    AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
+    s->smem_limit = (size_t)optin - 1024;  // static shared memory of the kernel
+    AS_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    for (auto& q : s->problems) {
+        bool any = false;
+        for (auto& v : variants()) any = any || fits(v, q, precision, s->smem_limit);
+        if (!any)
+            return fail(AS_ERR_UNSUPPORTED,
+                        "instance N=" + std::to_string(q.n) + " M=" + std::to_string(q.m) +
+                            " K=" + std::to_string(q.k) + " exceeds every compiled launch shape");
+    }
+    AS_CUDA(s->queue.alloc(64 * sizeof(int)));
+    AS_CUDA(s->solved.alloc(sizeof(int) * s->problems.size()));
+    AS_CUDA(s->deadline.alloc(sizeof(unsigned long long)));
+    *out = s.release();
+    return AS_OK;
+}
+
+void as_solver_free(as_solver* s) { delete s; }
+
+int32_t as_solver_set_max_time(as_solver* s, double v) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (!(v > 0.0)) return fail(AS_ERR_BAD_INPUT, "Max time must be positive");
+    s->max_time = v; s->invalidate();
+    return AS_OK;
+}
+int32_t as_solver_set_max_steps(as_solver* s, int32_t v) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (v < 1) return fail(AS_ERR_BAD_INPUT, "Max iterations must be positive");
+    s->max_steps = v; s->invalidate();
+    return AS_OK;
+}
+int32_t as_solver_set_batch_size(as_solver* s, int32_t v) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (v < 1) return fail(AS_ERR_BAD_INPUT, "Batch size must be positive");
+    s->batch = v; s->invalidate();
+    return AS_OK;
+}
+int32_t as_solver_set_epsilon(as_solver* s, double v) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (!(v >= 1e-16 && v <= 1.0)) return fail(AS_ERR_BAD_INPUT, "epsilon must be between 1e-16 and 1");
+    s->eps = v; s->invalidate();
+    return AS_OK;
+}
+int32_t as_solver_set_wall_budget(as_solver* s, double v) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (!(v >= 0.0)) return fail(AS_ERR_BAD_INPUT, "wall budget must be >= 0");
+    s->wall_budget = v; s->invalidate();
+    return AS_OK;
+}
+int32_t as_solver_set_stop_on_first(as_solver* s, int32_t f) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    s->stop_on_first = f ? 1 : 0; s->invalidate();
+    return AS_OK;
+}
+int32_t as_solver_set_track_best(as_solver* s, int32_t f) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    s->track_best = f ? 1 : 0; s->invalidate();
+    return AS_OK;
+}
+
+namespace {
+
+// Record the trajectories' problems and state offsets (user order) and size the
+// state buffer.  Grouping by launch shape happens lazily in build_groups.
+int plan_units(as_solver* s, const int32_t* problem_index, int num_traj) {
+    if (num_traj <= 0 || !problem_index) return fail(AS_ERR_BAD_INPUT, "need at least one trajectory");
+    const int np = (int)s->problems.size();
+    for (int t = 0; t < num_traj; t++)
+        if (problem_index[t] < 0 || problem_index[t] >= np)
+            return fail(AS_ERR_BAD_INPUT, "problem index out of range");
+    s->num_traj = num_traj;
+    s->traj_problem.assign(problem_index, problem_index + num_traj);
+    s->traj_off.resize(num_traj);
+    s->traj_bits.resize(num_traj);
+    long long off = 0, bo = 0;
+    for (int t = 0; t < num_traj; t++) {
+        const auto& q = s->problems[problem_index[t]];
+        s->traj_off[t] = off;
+        off += q.n + q.m;
+        s->traj_bits[t] = bo;
+        bo += (q.n + 31) / 32;
+    }
+    s->total_values = off;
+    const size_t vb = s->precision == AS_PREC_F64 ? 8 : 4;
+    AS_CUDA(s->states.alloc((size_t)off * vb));
+    AS_CUDA(s->results.alloc(sizeof(UnitResult) * num_traj));
+    AS_CUDA(s->unit_inst.alloc(sizeof(int) * num_traj));
+    AS_CUDA(s->unit_state.alloc(sizeof(long long) * num_traj));
+    AS_CUDA(s->unit_bits.alloc(sizeof(long long) * num_traj));
+    AS_CUDA(s->best_bits.alloc(sizeof(uint32_t) * std::max<long long>(bo, 1)));
+    s->groups_dirty = true;
+    s->invalidate();
+    return AS_OK;
+}
+
+// Pick the launch shape of every problem (smallest CTA that holds it, or the forced
+// shape), order the trajectories by (shape, problem) and upload the unit tables.
+int build_groups(as_solver* s) {
+    const auto& vs = variants();
+    const int np = (int)s->problems.size();
+    const int num_traj = s->num_traj;
+    std::vector<int> pv(np, -1);
+    for (int p = 0; p < np; p++) {
+        const auto& q = s->problems[p];
+        long best = -1;
+        const int want = s->forced_bt ? s->forced_bt : preferred_bt(q);
+        for (int i = 0; i < (int)vs.size(); i++) {
+            const auto& v = vs[i];
+            if (!fits(v, q, s->precision, s->smem_limit)) continue;
+            if (s->forced_bt && v.bt != s->forced_bt) continue;
+            // closest CTA size to the preferred one, then the smallest KMAX that holds k
+            const long score = (long)std::abs(v.bt - want) * 1024 + v.kmax;
+            if (best < 0 || score < best) { best = score; pv[p] = i; }
+        }
+        if (pv[p] < 0)
+            return fail(AS_ERR_UNSUPPORTED, "no compiled launch shape fits problem " + std::to_string(p));
+    }
+    const auto& pi = s->traj_problem;
+    s->order.resize(num_traj);
+    for (int t = 0; t < num_traj; t++) s->order[t] = t;
+    std::stable_sort(s->order.begin(), s->order.end(), [&](int a, int b) {
+        const int va = pv[pi[a]], vb = pv[pi[b]];
+        if (va != vb) return va < vb;
+        return pi[a] < pi[b];
+    });
+    s->groups.clear();
+    for (int u = 0; u < num_traj;) {
+        const int v = pv[pi[s->order[u]]];
+        int e = u;
+        while (e < num_traj && pv[pi[s->order[e]]] == v) e++;
+        s->groups.push_back({v, u, e});
+        u = e;
+    }
+    std::vector<int> ui(num_traj);
+    std::vector<long long> us(num_traj), ub(num_traj);
+    for (int u = 0; u < num_traj; u++) {
+        ui[u] = pi[s->order[u]];
+        us[u] = s->traj_off[s->order[u]];
+        ub[u] = s->traj_bits[s->order[u]];
+    }
+    if (s->groups.size() + 1 > s->queue.bytes / sizeof(int))
+        AS_CUDA(s->queue.alloc(sizeof(int) * (s->groups.size() + 1)));
+    AS_CUDA(cudaMemcpy(s->unit_inst.p, ui.data(), sizeof(int) * num_traj, cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(s->unit_state.p, us.data(), sizeof(long long) * num_traj, cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(s->unit_bits.p, ub.data(), sizeof(long long) * num_traj, cudaMemcpyHostToDevice));
+    s->groups_dirty = false;
+    s->invalidate();
+    return AS_OK;
+}
+
+template <typename SRC>
+int set_states_host(as_solver* s, const int32_t* pi, int nt, const SRC* src) {
+    if (!s || !src) return fail(AS_ERR_BAD_INPUT, "as_solver_set_states: null argument");
+    AS_CUDA(cudaSetDevice(s->device));
+    int r = plan_units(s, pi, nt);
+    if (r) return r;
+    const size_t n = (size_t)s->total_values;
+    if (s->precision == AS_PREC_F64) {
+        if (sizeof(SRC) == 8) {
+            AS_CUDA(cudaMemcpyAsync(s->states.p, src, n * 8, cudaMemcpyHostToDevice, s->stream));
+        } else {
+            std::vector<double> tmp(src, src + n);
+            AS_CUDA(cudaMemcpyAsync(s->states.p, tmp.data(), n * 8, cudaMemcpyHostToDevice, s->stream));
+            AS_CUDA(cudaStreamSynchronize(s->stream));
+        }
+    } else {
+        if (sizeof(SRC) == 4) {
+            AS_CUDA(cudaMemcpyAsync(s->states.p, src, n * 4, cudaMemcpyHostToDevice, s->stream));
+        } else {
+            std::vector<float> tmp(src, src + n);
+            AS_CUDA(cudaMemcpyAsync(s->states.p, tmp.data(), n * 4, cudaMemcpyHostToDevice, s->stream));
+            AS_CUDA(cudaStreamSynchronize(s->stream));
+        }
+    }
+    return AS_OK;
+}
+
+int record_solve(as_solver* s, cudaStream_t st) {
+    const auto& vs = variants();
+    AS_CUDA(cudaMemsetAsync(s->queue.p, 0, s->queue.bytes, st));
+    AS_CUDA(cudaMemsetAsync(s->solved.p, 0, s->solved.bytes, st));
+    const bool have_deadline = s->wall_budget > 0.0;
+    if (have_deadline) {
+        stamp_deadline_kernel<<<1, 1, 0, st>>>(s->deadline.as<unsigned long long>(),
+                                               (unsigned long long)(s->wall_budget * 1e9));
+        AS_CUDA(cudaGetLastError());
+    }
+    for (size_t g = 0; g < s->groups.size(); g++) {
+        const auto& G = s->groups[g];
+        const Variant& v = vs[G.variant];
+        size_t smem = 0;
+        for (int u = G.u0; u < G.u1; u++) {
+            const auto& q = s->problems[s->traj_problem[s->order[u]]];
+            smem = std::max(smem, solver_smem(v, q));
+        }
+        AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 0;
+        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.fn, v.bt, smem));
+        if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
+        const int units = G.u1 - G.u0;
+        const int ctas = std::min(units, s->sm_count * occ);
+        SolveParams P;
+        P.inst = s->pool.inst.as<DevInstance>();
+        P.unit_inst = s->unit_inst.as<int>() + G.u0;
+        P.unit_state = s->unit_state.as<long long>() + G.u0;
+        P.states = s->states.p;
+        P.results = s->results.as<UnitResult>() + G.u0;
+        P.queue_head = s->queue.as<int>() + g;
+        P.inst_solved = s->solved.as<int>();
+        P.best_bits = s->track_best ? s->best_bits.as<uint32_t>() : nullptr;
+        P.unit_bits = s->unit_bits.as<long long>() + G.u0;
+        P.num_units = units;
+        P.maxsteps = s->max_steps;
+        P.batch = s->batch;
+        P.stop_on_first = s->stop_on_first;
+        P.eps = s->eps;
+        P.tmax = s->max_time;
+        P.deadline = have_deadline ? s->deadline.as<unsigned long long>() : nullptr;
+        void* args[] = {&P};
+        AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(v.bt), args, smem, st));
+        s->last_bt = v.bt; s->last_ctas = ctas; s->last_smem = (int)smem; s->last_occ = occ;
+    }
+    return AS_OK;
+}
+
+}  // namespace
+
+int32_t as_solver_set_states_f64(as_solver* s, const int32_t* pi, int32_t nt, const double* st) {
+    return set_states_host<double>(s, pi, nt, st);
+}
+int32_t as_solver_set_states_f32(as_solver* s, const int32_t* pi, int32_t nt, const float* st) {
+    return set_states_host<float>(s, pi, nt, st);
+}
+int32_t as_solver_set_states_device(as_solver* s, const int32_t* pi, int32_t nt, const void* src,
+                                    void* stream) {
+    if (!s || !src) return fail(AS_ERR_BAD_INPUT, "as_solver_set_states_device: null argument");
+    AS_CUDA(cudaSetDevice(s->device));
+    int r = plan_units(s, pi, nt);
+    if (r) return r;
+    const size_t vb = s->precision == AS_PREC_F64 ? 8 : 4;
+    AS_CUDA(cudaMemcpyAsync(s->states.p, src, (size_t)s->total_values * vb, cudaMemcpyDeviceToDevice,
+                            stream ? (cudaStream_t)stream : s->stream));
+    if (stream) AS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return AS_OK;
+}
+
+int32_t as_solver_solve_async(as_solver* s, void* stream) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (s->num_traj <= 0) return fail(AS_ERR_NO_PROBLEM, "no trajectories set (as_solver_set_states_*)");
+    AS_CUDA(cudaSetDevice(s->device));
+    if (s->groups_dirty) {
+        int r = build_groups(s);
+        if (r) return r;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    if (st != s->stream) return record_solve(s, st);
+    if (!s->graph_valid) {
+        if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+        cudaGraph_t g = nullptr;
+        AS_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        int r = record_solve(s, s->stream);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (r) { if (g) cudaGraphDestroy(g); return r; }
+        if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        s->graph_valid = true;
+    }
+    AS_CUDA(cudaGraphLaunch(s->graph, s->stream));
+    return AS_OK;
+}
+
+int32_t as_solver_sync(as_solver* s) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    AS_CUDA(cudaStreamSynchronize(s->stream));
+    return AS_OK;
+}
+
+int32_t as_solver_solve(as_solver* s) {
+    int r = as_solver_solve_async(s, nullptr);
+    if (r) return r;
+    return as_solver_sync(s);
+}
+
+int32_t as_solver_get_results(as_solver* s, int32_t* status, double* time, int32_t* steps, int32_t* rhs,
+                              int32_t* attempts, int32_t* violations, int32_t* min_violations,
+                              double* last_step) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (s->num_traj <= 0) return fail(AS_ERR_NO_PROBLEM, "no trajectories set");
+    std::vector<UnitResult> r(s->num_traj);
+    AS_CUDA(cudaSetDevice(s->device));
+    AS_CUDA(cudaMemcpyAsync(r.data(), s->results.p, sizeof(UnitResult) * s->num_traj, cudaMemcpyDeviceToHost,
+                            s->stream));
+    AS_CUDA(cudaStreamSynchronize(s->stream));
+    for (int u = 0; u < s->num_traj; u++) {
+        const int t = s->order[u];
+        if (status) status[t] = r[u].status;
+        if (time) time[t] = r[u].time;
+        if (steps) steps[t] = r[u].steps;
+        if (rhs) rhs[t] = r[u].rhs;
+        if (attempts) attempts[t] = r[u].attempts;
+        if (violations) violations[t] = r[u].viol;
+        if (min_violations) min_violations[t] = r[u].min_viol;
+        if (last_step) last_step[t] = r[u].hdid;
+    }
+    return AS_OK;
+}
+
+namespace {
+template <typename DST>
+int get_states(as_solver* s, DST* out) {
+    if (!s || !out) return fail(AS_ERR_BAD_INPUT, "as_solver_get_states: null argument");
+    if (s->num_traj <= 0) return fail(AS_ERR_NO_PROBLEM, "no trajectories set");
+    AS_CUDA(cudaSetDevice(s->device));
+    const size_t n = (size_t)s->total_values;
+    const size_t vb = s->precision == AS_PREC_F64 ? 8 : 4;
+    if (vb == sizeof(DST)) {
+        AS_CUDA(cudaMemcpyAsync(out, s->states.p, n * vb, cudaMemcpyDeviceToHost, s->stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+    } else if (vb == 8) {
+        std::vector<double> tmp(n);
+        AS_CUDA(cudaMemcpyAsync(tmp.data(), s->states.p, n * 8, cudaMemcpyDeviceToHost, s->stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+        for (size_t i = 0; i < n; i++) out[i] = (DST)tmp[i];
+    } else {
+        std::vector<float> tmp(n);
+        AS_CUDA(cudaMemcpyAsync(tmp.data(), s->states.p, n * 4, cudaMemcpyDeviceToHost, s->stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+        for (size_t i = 0; i < n; i++) out[i] = (DST)tmp[i];
+    }
+    return AS_OK;
+}
+}  // namespace
+
+int32_t as_solver_get_states_f64(as_solver* s, double* out) { return get_states<double>(s, out); }
+int32_t as_solver_get_states_f32(as_solver* s, float* out) { return get_states<float>(s, out); }
+const void* as_solver_states_device(as_solver* s) { return s ? s->states.p : nullptr; }
+
+int32_t as_solver_get_best_assignment(as_solver* s, int32_t traj, uint32_t* bits) {
+    if (!s || !bits) return fail(AS_ERR_BAD_INPUT, "as_solver_get_best_assignment: null argument");
+    if (traj < 0 || traj >= s->num_traj) return fail(AS_ERR_BAD_INPUT, "trajectory index out of range");
+    if (!s->track_best) return fail(AS_ERR_BAD_INPUT, "best-assignment tracking is off");
+    const auto& q = s->problems[s->traj_problem[traj]];
+    AS_CUDA(cudaSetDevice(s->device));
+    AS_CUDA(cudaMemcpyAsync(bits, s->best_bits.as<uint32_t>() + s->traj_bits[traj],
+                            sizeof(uint32_t) * ((q.n + 31) / 32), cudaMemcpyDeviceToHost, s->stream));
+    AS_CUDA(cudaStreamSynchronize(s->stream));
+    return AS_OK;
+}
+
+int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas, int32_t* smem_bytes,
+                                   int32_t* ctas_per_sm) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (threads) *threads = s->last_bt;
+    if (ctas) *ctas = s->last_ctas;
+    if (smem_bytes) *smem_bytes = s->last_smem;
+    if (ctas_per_sm) *ctas_per_sm = s->last_occ;
+    return AS_OK;
+}
+
+int32_t as_solver_force_threads(as_solver* s, int32_t threads) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (threads != 0) {
+        bool any = false;
+        for (auto& v : variants()) any = any || (v.precision == s->precision && v.bt == threads);
+        if (!any) return fail(AS_ERR_UNSUPPORTED, "no compiled variant with that CTA size");
+    }
+    s->forced_bt = threads;
+    s->groups_dirty = true;
+    s->invalidate();
+    return AS_OK;
+}

@@ -1,0 +1,394 @@
+// Kernels of the AnalogSAT B200 hot path.
+//
+//  solve_kernel    persistent RK45 (Cash-Karp) integrator: one CTA per trajectory,
+//                  work units popped from a global counter (dynamic refill), spins
+//                  and clause contributions staged in shared memory, all RK stage
+//                  vectors held in registers (thread c owns clauses c, c+BT, ... and
+//                  variables c, c+BT, ...), batched clause check and early exit on
+//                  device.  Replaces SatSolver::DoSolve + CpuRungeKutta::Step/rkqs/
+//                  rkck + CpuSat::GetDerivatives/GetClauseViolationCount
+//                  (AnalogSAT/solver/SatSolver.h:273-355,
+//                  AnalogSAT/cpu_sat/CpuRungeKutta.cpp:66-100,181-267,
+//                  AnalogSAT/cpu_sat/CpuSat.cpp:65-94,136-173,199-241).
+//  rhs_batch_kernel   standalone RHS over many trajectories whose state lives in
+//                  HBM (ISat::GetDerivatives, AnalogSAT/solver/IODE.h).
+//  viol_batch_kernel  exact unsat counts for many states (ISat::GetClauseViolationCount).
+#pragma once
+
+#include <climits>
+#include "as_device.cuh"
+
+namespace asb {
+
+enum : int {
+    SAT_SOLUTION_FOUND = 0,
+    SAT_UNDERFLOW = 1,
+    SAT_ODE_INTERRUPTED = 2,
+    SAT_MAXTIME_REACHED = 3,
+    SAT_MAXITER_REACHED = 4,
+    SAT_UNKNOWN = 5,
+};
+
+struct UnitResult {
+    double time;      // integrated analog time
+    double hdid;      // last accepted step size
+    int status;       // SatResult code
+    int steps;        // accepted steps (SatSolver counting: whole batches)
+    int attempts;     // attempted steps incl. rejections
+    int rhs;          // RHS evaluations
+    int viol;         // unsat count at the last check
+    int min_viol;     // smallest unsat count seen at any check
+    int pad0, pad1;
+};
+
+struct SolveParams {
+    const DevInstance* inst;     // [num_instances]
+    const int* unit_inst;        // [num_units]
+    const long long* unit_state; // [num_units] element offset of the unit's public state
+    void* states;                // public layout [s_1..s_N, a_1..a_M] per unit (T)
+    UnitResult* results;         // [num_units]
+    int* queue_head;             // work counter, zero before launch
+    int* inst_solved;            // [num_instances] first-solution flags
+    uint32_t* best_bits;         // optional: per unit ceil(N/32) words, assignment at min_viol
+    const long long* unit_bits;  // [num_units] word offset into best_bits
+    int num_units;
+    int maxsteps;
+    int batch;
+    int stop_on_first;           // stop all trajectories of an instance at its first solution
+    double eps;
+    double tmax;
+    const unsigned long long* deadline;  // %globaltimer deadline (device word); null = none
+};
+
+// Cash-Karp tableau and NR step controller (AnalogSAT/cpu_sat/CpuRungeKutta.h:72-112).
+namespace ck {
+constexpr double TINY = 1e-20, SAFETY = 0.9, PGROW = -0.2, PSHRNK = -0.25, ERRCON = 1.89e-4,
+                 HFACTOR = 0.1;
+constexpr double b21 = 0.2, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0, b41 = 0.3, b42 = -0.9, b43 = 1.2,
+                 b51 = -11.0 / 54.0, b52 = 2.5, b53 = -70.0 / 27.0, b54 = 35.0 / 27.0,
+                 b61 = 1631.0 / 55296.0, b62 = 175.0 / 512.0, b63 = 575.0 / 13824.0,
+                 b64 = 44275.0 / 110592.0, b65 = 253.0 / 4096.0, c1 = 37.0 / 378.0,
+                 c3 = 250.0 / 621.0, c4 = 125.0 / 594.0, c6 = 512.0 / 1771.0,
+                 dc5 = -277.0 / 14336.0, dc1 = c1 - 2825.0 / 27648.0, dc3 = c3 - 18575.0 / 48384.0,
+                 dc4 = c4 - 13525.0 / 55296.0, dc6 = c6 - 0.25;
+}  // namespace ck
+
+// Stage input y_S = x + h * sum_j b_Sj k_j in the reference's expression order.
+template <int S, typename T>
+__device__ __forceinline__ T stage_in(T x, T k1, T k2, T k3, T k4, T k5, T h) {
+    using A = Arith<T>;
+    if constexpr (S == 1) return x;
+    if constexpr (S == 2) return A::add(x, A::mul(A::mul(T(ck::b21), h), k1));
+    if constexpr (S == 3) return A::add(x, A::mul(h, A::add(A::mul(T(ck::b31), k1), A::mul(T(ck::b32), k2))));
+    if constexpr (S == 4)
+        return A::add(x, A::mul(h, A::add(A::add(A::mul(T(ck::b41), k1), A::mul(T(ck::b42), k2)),
+                                          A::mul(T(ck::b43), k3))));
+    if constexpr (S == 5)
+        return A::add(x, A::mul(h, A::add(A::add(A::add(A::mul(T(ck::b51), k1), A::mul(T(ck::b52), k2)),
+                                                 A::mul(T(ck::b53), k3)),
+                                          A::mul(T(ck::b54), k4))));
+    if constexpr (S == 6)
+        return A::add(
+            x, A::mul(h, A::add(A::add(A::add(A::add(A::mul(T(ck::b61), k1), A::mul(T(ck::b62), k2)),
+                                              A::mul(T(ck::b63), k3)),
+                                       A::mul(T(ck::b64), k4)),
+                                A::mul(T(ck::b65), k5))));
+    return x;
+}
+
+// xnew = x + h (c1 k1 + c3 k3 + c4 k4 + c6 k6)
+template <typename T>
+__device__ __forceinline__ T rk_new(T x, T k1, T k3, T k4, T k6, T h) {
+    using A = Arith<T>;
+    return A::add(x, A::mul(h, A::add(A::add(A::add(A::mul(T(ck::c1), k1), A::mul(T(ck::c3), k3)),
+                                             A::mul(T(ck::c4), k4)),
+                                      A::mul(T(ck::c6), k6))));
+}
+
+// |xerr / xscal| in FP64 (the controller's error norm is always accumulated in FP64).
+// xscal = |x| + |k1 h0| + TINY (CpuRungeKutta.cpp:85); in log space the a-block uses
+// 1 + |k1 h0| + TINY, i.e. the reference's relative error of a.
+template <typename T>
+__device__ __forceinline__ double rk_err_ratio(T x, T k1, T k3, T k4, T k5, T k6, double h,
+                                               double h0, bool unit_scale) {
+    using D = Arith<double>;
+    const double e = D::mul(
+        h, D::add(D::add(D::add(D::add(D::mul(ck::dc1, (double)k1), D::mul(ck::dc3, (double)k3)),
+                                D::mul(ck::dc4, (double)k4)),
+                         D::mul(ck::dc5, (double)k5)),
+                  D::mul(ck::dc6, (double)k6)));
+    const double xa = unit_scale ? 1.0 : fabs((double)x);
+    if constexpr (sizeof(T) == 8) {
+        const double sc = D::add(D::add(xa, fabs(D::mul((double)k1, h0))), ck::TINY);
+        return fabs(__ddiv_rn(e, sc));
+    } else {
+        // FP32 state: the cancellation-prone error sum and the scale are FP64; their
+        // quotient only feeds a tolerance test, so it is formed in FP32 (an IEEE FP64
+        // divide here costs more registers than the whole RHS).
+        const double sc = xa + fabs((double)(k1 * (T)h0)) + ck::TINY;
+        return (double)fabsf(__fdiv_rn((float)e, (float)sc));
+    }
+}
+
+template <int BT>
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent solver kernel
+// ---------------------------------------------------------------------------
+// Shared-memory layout of one trajectory (E = n + m state elements, public order:
+// spins 0..n-1, then clause weights n..n+m-1):
+//   X, K1..K5   the RK stage vectors (state, k1..k5), E values each;
+//   sy          the stage's spin vector plus the sentinel slot sy[n] = -1;
+//   contrib     per-literal spin contributions, k * mp values.
+// Element e is owned by thread e % BT in every loop, so stage vectors need no
+// barriers; only sy and contrib are exchanged between threads.
+template <typename T>
+struct Stages {
+    T *X, *K1, *K2, *K3, *K4, *K5;
+};
+
+template <typename T>
+__host__ __device__ inline size_t solve_smem_values(int n, int m, int k, int mp) {
+    const size_t E = (size_t)((n + m + 3) & ~3);
+    return 6 * E + (size_t)((n + 1 + 3) & ~3) + (size_t)k * mp;
+}
+
+template <typename T, bool LOGA, int KMAX, int BT>
+struct Solver {
+    using A = Arith<T>;
+
+    // One RHS evaluation at stage S.  The stage input is formed on the fly from the
+    // stage vectors; the derivative lands in K_S, or for S == 6 is consumed at once
+    // into xnew (stored in K2, dead after the stage-6 input) and the error norm.
+    template <int S>
+    static __device__ __forceinline__ void eval(const DevInstance& I, T* sy, T* contrib, T knorm,
+                                                const Stages<T>& st, T hT, double h, double h0,
+                                                double& errmax) {
+        const int tid = threadIdx.x;
+        const int n = I.n;
+        for (int i = tid; i < n; i += BT)
+            sy[i] = stage_in<S>(st.X[i], st.K1[i], st.K2[i], st.K3[i], st.K4[i], st.K5[i], hT);
+        __syncthreads();
+        for (int m = tid; m < I.m; m += BT) {
+            const int e = n + m;
+            const T x = st.X[e];
+            const T y = stage_in<S>(x, st.K1[e], st.K2[e], st.K3[e], st.K4[e], st.K5[e], hT);
+            const T am = LOGA ? A::ex(y) : y;
+            const T d = clause_phase<T, LOGA, KMAX>(I, m, sy, contrib, am, knorm);
+            if constexpr (S == 1) st.K1[e] = d;
+            if constexpr (S == 2) st.K2[e] = d;
+            if constexpr (S == 3) st.K3[e] = d;
+            if constexpr (S == 4) st.K4[e] = d;
+            if constexpr (S == 5) st.K5[e] = d;
+            if constexpr (S == 6) {
+                const T k1 = st.K1[e], k3 = st.K3[e], k4 = st.K4[e];
+                errmax = fmax(errmax, rk_err_ratio<T>(x, k1, k3, k4, st.K5[e], d, h, h0, LOGA));
+                st.K2[e] = rk_new<T>(x, k1, k3, k4, d, hT);
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < n; i += BT) {
+            const T d = var_phase<T>(I, i, contrib);
+            if constexpr (S == 1) st.K1[i] = d;
+            if constexpr (S == 2) st.K2[i] = d;
+            if constexpr (S == 3) st.K3[i] = d;
+            if constexpr (S == 4) st.K4[i] = d;
+            if constexpr (S == 5) st.K5[i] = d;
+            if constexpr (S == 6) {
+                const T x = st.X[i], k1 = st.K1[i], k3 = st.K3[i], k4 = st.K4[i];
+                errmax = fmax(errmax, rk_err_ratio<T>(x, k1, k3, k4, st.K5[i], d, h, h0, false));
+                st.K2[i] = rk_new<T>(x, k1, k3, k4, d, hT);
+            }
+        }
+    }
+};
+
+template <typename T, bool LOGA, int KMAX, int BT>
+__global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel(SolveParams P) {
+    using A = Arith<T>;
+    using S = Solver<T, LOGA, KMAX, BT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red_d[BT / 32];
+    __shared__ int red_i[BT / 32];
+    __shared__ int s_unit, s_flag;
+    const int tid = threadIdx.x;
+
+    while (true) {
+        if (tid == 0) s_unit = atomicAdd(P.queue_head, 1);
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= P.num_units) break;
+        const int pidx = P.unit_inst[u];
+        const DevInstance I = P.inst[pidx];
+        const int n = I.n, E = I.n + I.m;
+        const int Ep = (E + 3) & ~3;
+        T* base = reinterpret_cast<T*>(smem_raw);
+        Stages<T> st{base, base + Ep, base + 2 * Ep, base + 3 * Ep, base + 4 * Ep, base + 5 * Ep};
+        T* sy = base + 6 * Ep;
+        T* contrib = sy + ((n + 1 + 3) & ~3);
+        T* G = reinterpret_cast<T*>(P.states) + P.unit_state[u];
+        const T knorm = (T)ldexp(1.0, -I.k);
+
+        // load the initial state (a -> ln a in log space)
+        for (int e = tid; e < E; e += BT) {
+            const T v = G[e];
+            st.X[e] = (LOGA && e >= n) ? A::lg(v) : v;
+            st.K1[e] = st.K2[e] = st.K3[e] = st.K4[e] = st.K5[e] = T(0);
+        }
+        if (tid == 0) sy[n] = T(-1);  // sentinel spin: padding literals are always FALSE
+
+        double t = 0.0, hnext = 1e-9, hdid = 0.0;
+        int steps = 0, attempts = 0, rhs = 0, viol = -1, minviol = INT_MAX;
+        int status = SAT_UNKNOWN;
+
+        // an instance already solved by another trajectory (stop_on_first) is skipped
+        if (tid == 0) s_flag = P.stop_on_first ? (atomicAdd(P.inst_solved + pidx, 0) != 0) : 0;
+        __syncthreads();
+        if (s_flag) status = SAT_ODE_INTERRUPTED;
+
+        while (status == SAT_UNKNOWN && t < P.tmax && steps < P.maxsteps) {
+            bool underflow = false;
+            int taken = 0;
+            for (int b = 0; b < P.batch; b++) {
+                // ---- CpuRungeKutta::Step, count = 1 ----
+                double dummy = 0.0;
+                S::template eval<1>(I, sy, contrib, knorm, st, T(0), 0.0, 0.0, dummy);
+                rhs++;
+                const double h0 = hnext;
+                double h = hnext, ermax = 0.0;
+                while (true) {
+                    const T hT = (T)h;
+                    double em = 0.0;
+                    S::template eval<2>(I, sy, contrib, knorm, st, hT, h, h0, em);
+                    S::template eval<3>(I, sy, contrib, knorm, st, hT, h, h0, em);
+                    S::template eval<4>(I, sy, contrib, knorm, st, hT, h, h0, em);
+                    S::template eval<5>(I, sy, contrib, knorm, st, hT, h, h0, em);
+                    S::template eval<6>(I, sy, contrib, knorm, st, hT, h, h0, em);
+                    rhs += 5;
+                    attempts++;
+                    ermax = __ddiv_rn(block_max<BT>(em, red_d), P.eps);
+                    if (ermax <= 1.0) break;
+                    const double htemp = __dmul_rn(__dmul_rn(ck::SAFETY, h), pow(ermax, ck::PSHRNK));
+                    h = fmax(htemp, __dmul_rn(ck::HFACTOR, h));
+                    if (__dadd_rn(t, h) == t) { underflow = true; break; }
+                }
+                if (underflow) break;
+                hnext = ermax > ck::ERRCON ? __dmul_rn(__dmul_rn(ck::SAFETY, h), pow(ermax, ck::PGROW))
+                                           : __dmul_rn(5.0, h);
+                hdid = h;
+                t = __dadd_rn(t, h);
+                taken++;
+                // accept: xnew (held in K2) becomes the state
+                T* tmp = st.X; st.X = st.K2; st.K2 = tmp;
+            }
+            if (underflow) { status = SAT_UNDERFLOW; break; }
+            steps += taken;
+
+            // ---- CpuSat::GetClauseViolationCount on the accepted state ----
+            for (int i = tid; i < n; i += BT) sy[i] = st.X[i];
+            __syncthreads();
+            int cnt = 0;
+            for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX>(I, m, sy);
+            viol = block_sum<BT>(cnt, red_i);
+            if (viol < minviol) {
+                minviol = viol;
+                if (P.best_bits) {
+                    uint32_t* bits = P.best_bits + P.unit_bits[u];
+                    for (int i0 = tid & ~31; i0 < n; i0 += BT) {
+                        const int i = i0 + (tid & 31);
+                        const unsigned bal = __ballot_sync(0xffffffffu, i < n && sy[i < n ? i : 0] > T(0));
+                        if ((tid & 31) == 0) bits[i0 >> 5] = bal;
+                    }
+                }
+            }
+            if (viol == 0) {
+                status = SAT_SOLUTION_FOUND;
+                if (tid == 0 && P.stop_on_first) atomicExch(P.inst_solved + pidx, 1);
+                break;
+            }
+            if (tid == 0) {
+                int f = 0;
+                if (P.deadline && globaltimer_ns<BT>() >= *P.deadline) f = 1;
+                if (P.stop_on_first && atomicAdd(P.inst_solved + pidx, 0) != 0) f = 1;
+                s_flag = f;
+            }
+            __syncthreads();
+            if (s_flag) { status = SAT_ODE_INTERRUPTED; break; }
+        }
+        if (status == SAT_UNKNOWN) {
+            if (t >= P.tmax) status = SAT_MAXTIME_REACHED;
+            else if (steps >= P.maxsteps) status = SAT_MAXITER_REACHED;
+        }
+
+        // write back the final state in the public layout
+        for (int e = tid; e < E; e += BT) {
+            const T v = st.X[e];
+            G[e] = (LOGA && e >= n) ? A::ex(v) : v;
+        }
+        if (tid == 0) {
+            UnitResult r;
+            r.time = t; r.hdid = hdid; r.status = status; r.steps = steps; r.attempts = attempts;
+            r.rhs = rhs; r.viol = viol; r.min_viol = minviol == INT_MAX ? -1 : minviol;
+            r.pad0 = r.pad1 = 0;
+            P.results[u] = r;
+        }
+        __syncthreads();  // s_unit / shared buffers are reused by the next unit
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Standalone batched RHS: one CTA per trajectory, state in global memory.
+// ---------------------------------------------------------------------------
+template <typename T, bool LOGA, int KMAX, int BT>
+__global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* __restrict__ x,
+                                                        T* __restrict__ dxdt, int ntraj,
+                                                        long long stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sy = reinterpret_cast<T*>(smem_raw);
+    T* contrib = sy + ((I.n + 1 + 3) & ~3);
+    const int tid = threadIdx.x;
+    const T knorm = (T)ldexp(1.0, -I.k);
+    for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
+        const T* X = x + (long long)tr * stride;
+        T* D = dxdt + (long long)tr * stride;
+        for (int i = tid; i < I.n; i += BT) sy[i] = X[i];
+        if (tid == 0) sy[I.n] = T(-1);
+        __syncthreads();
+        for (int m = tid; m < I.m; m += BT) {
+            const T a = X[I.n + m];
+            D[I.n + m] = clause_phase<T, LOGA, KMAX>(I, m, sy, contrib, LOGA ? Arith<T>::ex(a) : a, knorm);
+        }
+        __syncthreads();
+        for (int i = tid; i < I.n; i += BT) D[i] = var_phase<T>(I, i, contrib);
+        __syncthreads();
+    }
+}
+
+// Exact unsat counts of many states: one CTA per state.
+template <typename T, int KMAX, int BT>
+__global__ void __launch_bounds__(BT) viol_batch_kernel(DevInstance I, const T* __restrict__ x,
+                                                         int* __restrict__ counts, int ntraj,
+                                                         long long stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int red_i[BT / 32];
+    T* sy = reinterpret_cast<T*>(smem_raw);
+    const int tid = threadIdx.x;
+    for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
+        const T* X = x + (long long)tr * stride;
+        for (int i = tid; i < I.n; i += BT) sy[i] = X[i];
+        if (tid == 0) sy[I.n] = T(-1);
+        __syncthreads();
+        int cnt = 0;
+        for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX>(I, m, sy);
+        cnt = block_sum<BT>(cnt, red_i);
+        if (tid == 0) counts[tr] = cnt;
+        __syncthreads();
+    }
+}
+
+}  // namespace asb

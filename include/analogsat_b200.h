@@ -1,0 +1,189 @@
+/*
+ * analogsat_b200.h -- C ABI of the B200 (sm_100a) AnalogSAT CTDS solver.
+ *
+ * The reference library's boundary is a C++ template API (AnalogSAT/solver/*.h):
+ * SatProblem + CnfReader/CnfWriter for the CNF, ISat (the ODE right-hand side and
+ * clause check), IODEInt (the RK45 integrator) and SatSolver (the run-to-solution
+ * loop).  This header exports that functionality as plain `extern "C"` calls:
+ * opaque handles, plain pointers and sizes, int32 status codes, no exceptions.
+ * Each declaration names the reference interface it replaces (file:line, relative
+ * to the reference project root).
+ *
+ * Conventions
+ *  - Every function returns AS_OK (0) or a negative AS_ERR_* code, except the
+ *    solve calls, which return AS_OK and report per-trajectory SatResult codes.
+ *    as_last_error() gives the message of the last failure on the calling thread.
+ *  - Public state vectors use the reference order [s_1..s_N, a_1..a_M]
+ *    (AnalogSAT/solver/ISatState.h:72-127), a in linear space.
+ *  - `stream` arguments are cudaStream_t values passed as void* (NULL = the
+ *    legacy default stream).  Device-pointer calls are asynchronous on it.
+ *  - Handles are not thread-safe; distinct handles may be used concurrently.
+ *    There is no process-global device state (the reference keeps its RK45
+ *    constants and buffer pointers in __constant__ symbols,
+ *    AnalogSAT/cuda_sat/CudaRungeKutta.cu:42-45, so it allows one integrator
+ *    per process).
+ */
+#ifndef ANALOGSAT_B200_H
+#define ANALOGSAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------------
+ * SatResult values (AnalogSAT/solver/SatResult.h:24-32), returned per trajectory. */
+#define AS_SAT_SOLUTION_FOUND 0
+#define AS_SAT_UNDERFLOW 1
+#define AS_SAT_ODE_INTERRUPTED 2
+#define AS_SAT_MAXTIME_REACHED 3
+#define AS_SAT_MAXITER_REACHED 4
+#define AS_SAT_UNKNOWN 5
+
+/* call status (the reference throws: invalid_argument for bad parameters,
+ * SatSolver.h:137,147,157 and CpuRungeKutta.cpp:129; runtime_error when no problem
+ * is set, CpuSat.cpp:67; CudaSafe on CUDA errors, CudaUtils.cu:27-44) */
+#define AS_OK 0
+#define AS_ERR_BAD_INPUT (-1)
+#define AS_ERR_CUDA (-2)
+#define AS_ERR_NO_PROBLEM (-3)
+#define AS_ERR_UNSUPPORTED (-4)
+#define AS_ERR_IO (-5)
+
+/* numeric modes */
+#define AS_PREC_F32_LOGA 0 /* FP32 state, a_m held as ln a_m, FP64 error norm + time */
+#define AS_PREC_F64 1      /* FP64 state, linear a_m: bit-for-bit the reference RHS */
+
+typedef struct as_problem as_problem;
+typedef struct as_solver as_solver;
+
+/* Message of the last failed call on this thread ("" if none). Returns its length. */
+int32_t as_last_error(char* buf, int32_t buf_len);
+
+/* Library / device information: number of SMs of `device`, or a negative error. */
+int32_t as_device_sm_count(int32_t device);
+
+/* ---- problems (SatProblem, AnalogSAT/problem/SatProblem.h:26-63) ----------- */
+
+/* SatProblem::AddClauses(literals, lengths) (SatProblem.cpp:64-95): zero literals
+ * are filtered, empty clauses dropped, N = max |literal|, K = max clause length. */
+int32_t as_problem_create(const int32_t* literals, const int32_t* lengths, int32_t num_clauses,
+                          as_problem** out);
+
+/* CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141); msg receives the reader's message. */
+int32_t as_problem_read_cnf(const char* path, as_problem** out, char* msg, int32_t msg_len);
+
+/* CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74). */
+int32_t as_problem_write_cnf(const as_problem* p, const char* path);
+
+/* SatProblem::Get_N / Get_M / Get_K (SatProblem.h:58-60). */
+int32_t as_problem_get_nmk(const as_problem* p, int32_t* n, int32_t* m, int32_t* k);
+
+/* SatProblem::GetAllClauses (SatProblem.cpp:104-110): literals must hold the total
+ * literal count (as_problem_num_literals), lengths M entries. */
+int32_t as_problem_num_literals(const as_problem* p);
+int32_t as_problem_get_clauses(const as_problem* p, int32_t* literals, int32_t* lengths);
+
+void as_problem_free(as_problem* p);
+
+/* ---- device primitives (ISat, AnalogSAT/solver/ISat.h:31-87) -------------- */
+
+/* ISat::GetDerivatives over `num_states` states at once (CpuSat.cpp:65-94,
+ * CudaSat1.cu:501-531).  x and dxdt are DEVICE pointers to num_states public-layout
+ * vectors of N+M values each (FP32).  logspace = 1: the a-block of x holds
+ * u = ln a and receives du/dt = K^2. */
+int32_t as_rhs_f32(as_problem* p, const float* x, float* dxdt, int32_t num_states,
+                   int32_t logspace, void* stream);
+/* FP64 variant, linear a: bit-identical to CpuSat<double>::GetDerivatives. */
+int32_t as_rhs_f64(as_problem* p, const double* x, double* dxdt, int32_t num_states, void* stream);
+
+/* ISat::GetClauseViolationCount over many states (CpuSat.cpp:136-173,
+ * CudaSat1.cu:484-498).  x: DEVICE pointer to num_states public vectors (only the
+ * first N entries of each, the spins, are read); counts: DEVICE int32[num_states]. */
+int32_t as_violations_f32(as_problem* p, const float* x, int32_t* counts, int32_t num_states,
+                          void* stream);
+int32_t as_violations_f64(as_problem* p, const double* x, int32_t* counts, int32_t num_states,
+                          void* stream);
+
+/* ---- batched solver (SatSolver<T,S>, AnalogSAT/solver/SatSolver.h:41-356) -- */
+
+/* SatSolver(ISat, IODEInt) + SetProblem (SatSolver.h:54-71, 207-218) for a batch of
+ * instances.  The solver keeps its own device copy of every problem (the handles
+ * may be freed afterwards).  precision: AS_PREC_*.  device: CUDA ordinal (-1 =
+ * current). */
+int32_t as_solver_create(const as_problem* const* problems, int32_t num_problems,
+                         int32_t precision, int32_t device, as_solver** out);
+void as_solver_free(as_solver* s);
+
+/* SatSolver setters (SatSolver.h:133-160; defaults maxTime 100, maxSteps 1e5,
+ * batchSize 20 at 60-62) and CpuRungeKutta::SetEpsilon (CpuRungeKutta.cpp:126-131,
+ * default 1e-4, valid range [1e-16, 1]). */
+int32_t as_solver_set_max_time(as_solver* s, double max_time);
+int32_t as_solver_set_max_steps(as_solver* s, int32_t max_steps);
+int32_t as_solver_set_batch_size(as_solver* s, int32_t batch_size);
+int32_t as_solver_set_epsilon(as_solver* s, double eps);
+/* Wall-clock budget per solve call in seconds (0 = none).  Trajectories still running
+ * when it expires stop with AS_SAT_ODE_INTERRUPTED -- the reference frontend gets the
+ * same result from its callback returning false (Frontend/src/bench_runner.cpp:225-229). */
+int32_t as_solver_set_wall_budget(as_solver* s, double seconds);
+/* 1: the first trajectory that solves an instance stops that instance's other
+ * trajectories (AS_SAT_ODE_INTERRUPTED).  0 (default): every trajectory runs on. */
+int32_t as_solver_set_stop_on_first(as_solver* s, int32_t flag);
+/* 1: keep, per trajectory, the Boolean assignment with the fewest unsat clauses
+ * seen at any check (MAXSAT runs); read it with as_solver_get_best_assignment. */
+int32_t as_solver_set_track_best(as_solver* s, int32_t flag);
+
+/* SatSolver::SetSatState (SatSolver.h:183-192) for a set of trajectories.  Trajectory
+ * t solves problem problem_index[t] from states + offset_t, where the host arrays are
+ * concatenated public vectors (N_p + M_p values each, in trajectory order). */
+int32_t as_solver_set_states_f64(as_solver* s, const int32_t* problem_index, int32_t num_traj,
+                                 const double* states);
+int32_t as_solver_set_states_f32(as_solver* s, const int32_t* problem_index, int32_t num_traj,
+                                 const float* states);
+/* Same with the states already on the device (in the solver's precision:
+ * float for AS_PREC_F32_LOGA, double for AS_PREC_F64), copied device-to-device. */
+int32_t as_solver_set_states_device(as_solver* s, const int32_t* problem_index, int32_t num_traj,
+                                    const void* states_dev, void* stream);
+
+/* SatSolver::Solve (SatSolver.h:162-165, DoSolve 273-355) for every trajectory, in
+ * one persistent launch.  Blocks until done.  Per-trajectory results via
+ * as_solver_get_results. */
+int32_t as_solver_solve(as_solver* s);
+/* Asynchronous form: enqueue on `stream`; completion via as_solver_sync. */
+int32_t as_solver_solve_async(as_solver* s, void* stream);
+int32_t as_solver_sync(as_solver* s);
+
+/* Per-trajectory statistics (SatSolver getters, SatSolver.h:77-130): any pointer may
+ * be NULL.  status: SatResult code; time: GetElapsedTime; steps: GetStepCount; rhs:
+ * GetRhsCount; attempts: IODEInt::GetAttemptCount; violations:
+ * GetLastClauseViolationCount; min_violations: smallest count seen; last_step:
+ * GetLastStepSize. */
+int32_t as_solver_get_results(as_solver* s, int32_t* status, double* time, int32_t* steps,
+                              int32_t* rhs, int32_t* attempts, int32_t* violations,
+                              int32_t* min_violations, double* last_step);
+
+/* SatSolver::GetSatState().CopyTo (SatSolver.h:168-169): final public states of all
+ * trajectories, concatenated as in as_solver_set_states_*. */
+int32_t as_solver_get_states_f64(as_solver* s, double* states);
+int32_t as_solver_get_states_f32(as_solver* s, float* states);
+/* Device pointer of the solver's state buffer (solver precision), for zero-copy reads. */
+const void* as_solver_states_device(as_solver* s);
+
+/* Best assignment of trajectory t (needs as_solver_set_track_best(s, 1) before the
+ * solve): bits[w] bit b = variable 32w+b+1 TRUE.  bits holds ceil(N/32) words. */
+int32_t as_solver_get_best_assignment(as_solver* s, int32_t traj, uint32_t* bits);
+
+/* Launch shape of the last solve's final launch group: threads per CTA, CTAs
+ * launched, dynamic shared memory per CTA and resident CTAs per SM. */
+int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas, int32_t* smem_bytes,
+                                   int32_t* ctas_per_sm);
+/* Force the CTA size (128, 256, 512 or 1024 threads) of the next solves; 0 restores
+ * the automatic choice (about four clauses per thread).  Used by the autotuner.
+ * Fails with AS_ERR_UNSUPPORTED when no compiled variant has that size. */
+int32_t as_solver_force_threads(as_solver* s, int32_t threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANALOGSAT_B200_H */

@@ -1,0 +1,127 @@
+"""The oracle (oracle/ctds_oracle.c) pinned against the reference solver's own outputs.
+
+The golden fixtures were produced by the reference AnalogSAT CPU code itself
+(tests/golden/make_golden.py); the C restatement must reproduce them bit for bit
+in FP64 (same expression order, no FMA contraction).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import REF_SO
+
+TAGS_RHS = ["p50", "mix", "r4", "k12", "p200", "p1000"]
+TAGS_TRAJ = ["p50", "mix", "r4", "p200", "p1000"]
+
+
+def _problem(oracle, golden, tag):
+    p = oracle.problem(golden[f"{tag}/literals"], golden[f"{tag}/lengths"])
+    assert (p.n, p.m, p.k) == tuple(golden[f"{tag}/nmk"])
+    return p
+
+
+@pytest.mark.parametrize("tag", TAGS_RHS)
+def test_rhs_bit_exact(oracle, golden, tag):
+    p = _problem(oracle, golden, tag)
+    for x, ref in zip(golden[f"{tag}/rhs_states"], golden[f"{tag}/rhs_f64"]):
+        d = oracle.rhs(p, x)
+        assert np.array_equal(d, ref), np.abs(d - ref).max()
+
+
+@pytest.mark.parametrize("tag", TAGS_RHS)
+def test_violation_counts_exact(oracle, golden, tag):
+    p = _problem(oracle, golden, tag)
+    for x, ref in zip(golden[f"{tag}/rhs_states"], golden[f"{tag}/viol"]):
+        assert oracle.violations(p, x) == ref
+
+
+@pytest.mark.parametrize("tag", TAGS_TRAJ)
+def test_trajectory_bit_exact(oracle, golden, tag):
+    p = _problem(oracle, golden, tag)
+    t = golden[f"{tag}/traj_time"]
+    tr = oracle.steps(p, golden[f"{tag}/traj_ic"], float(golden[f"{tag}/traj_eps"][0]), len(t))
+    assert tr["n"] == len(t)
+    assert np.array_equal(tr["time"], t)
+    assert np.array_equal(tr["h"], golden[f"{tag}/traj_h"])
+    assert np.array_equal(tr["rhs"], golden[f"{tag}/traj_rhs"])
+    assert np.array_equal(tr["attempts"], golden[f"{tag}/traj_attempts"])
+    assert np.array_equal(tr["states"][-1], golden[f"{tag}/traj_final"])
+    assert np.array_equal(tr["states"][len(t) // 2], golden[f"{tag}/traj_mid"])
+
+
+@pytest.mark.parametrize("tag", ["p50", "cfg1"])
+def test_solve_matches_reference(oracle, golden, tag):
+    p = _problem(oracle, golden, tag)
+    eps, batch, maxsteps, tmax = golden[f"{tag}/solve_params"]
+    for i, ic in enumerate(golden[f"{tag}/solve_ics"]):
+        r = oracle.solve(p, ic, eps=eps, tmax=tmax, maxsteps=int(maxsteps), batch=int(batch))
+        assert r["result"] == golden[f"{tag}/solve_result"][i]
+        assert r["steps"] == golden[f"{tag}/solve_steps"][i]
+        assert r["rhs"] == golden[f"{tag}/solve_rhs"][i]
+        assert r["time"] == golden[f"{tag}/solve_time"][i]
+        assert np.array_equal(r["state"], golden[f"{tag}/solve_final"][i])
+
+
+def test_solutions_verify_exactly(oracle, golden):
+    """Every SAT_SOLUTION_FOUND state satisfies all clauses (exact integer check)."""
+    from analogsat_b200.instances import is_satisfied
+    for tag in ["p50", "cfg1"]:
+        p = _problem(oracle, golden, tag)
+        for r, x in zip(golden[f"{tag}/solve_result"], golden[f"{tag}/solve_final"]):
+            if r == 0:
+                assert oracle.violations(p, x) == 0
+                assert is_satisfied(golden[f"{tag}/literals"], golden[f"{tag}/lengths"], x[: p.n] > 0)
+
+
+def test_planted_and_minisat_certificates(oracle, golden):
+    from analogsat_b200.instances import is_satisfied
+    for tag in ["p50", "p200", "p1000"]:
+        assert is_satisfied(golden[f"{tag}/literals"], golden[f"{tag}/lengths"],
+                            golden[f"{tag}/planted"].astype(bool))
+    assert golden["p50/minisat"][0] == 10
+    assert is_satisfied(golden["cfg1/literals"], golden["cfg1/lengths"],
+                        golden["cfg1/minisat_solution"].astype(bool))
+
+
+def test_logspace_same_ode(oracle, golden):
+    """Log-space a is the same ODE: du/dt = K^2 = (da/dt)/a, ds/dt unchanged."""
+    p = _problem(oracle, golden, "p200")
+    x = golden["p200/rhs_states"][0].copy()
+    x[p.n:] = np.linspace(0.5, 3.0, p.m)
+    d = oracle.rhs(p, x)
+    xl = x.copy(); xl[p.n:] = np.log(x[p.n:])
+    dl = oracle.rhs(p, xl, logspace=True)
+    np.testing.assert_allclose(dl[: p.n], d[: p.n], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(dl[p.n:], d[p.n:] / x[p.n:], rtol=1e-12, atol=1e-18)
+
+
+def test_logspace_trajectory_close(oracle, golden):
+    """Integrating ln a instead of a changes the discretisation only: over a short
+    horizon the two FP64 runs agree to the integration tolerance."""
+    p = _problem(oracle, golden, "p200")
+    ic = golden["p200/traj_ic"]
+    lin = oracle.steps(p, ic, 1e-6, 100)
+    lg = oracle.steps(p, ic, 1e-6, 100, logspace=True)
+    T = min(lin["time"][-1], lg["time"][-1])
+    # compare at matching step count; both integrate the same ODE within eps 1e-6
+    assert abs(lin["time"][-1] - lg["time"][-1]) / lin["time"][-1] < 0.05
+    assert T > 0
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference checker not built here")
+def test_oracle_vs_live_reference(oracle):
+    """Fresh instances from the reference makers: RHS and 50 steps bit-exact."""
+    from oracle import Reference
+    R = Reference()
+    rng = np.random.default_rng(5)
+    for kind, n, m, k, seed in [("planted", 60, 255, 3, 3), ("random", 33, 140, 4, 4),
+                                ("fast", 25, 60, 5, 5)]:
+        rp = R.make(kind, seed, n, m, k)
+        lits, lens = rp.export()
+        op = oracle.problem(lits, lens)
+        x = np.concatenate([rng.uniform(-1, 1, rp.n), rng.uniform(1, 2, rp.m)])
+        assert np.array_equal(R.rhs(rp, x), oracle.rhs(op, x))
+        a = R.steps(rp, x, 1e-6, 50)
+        b = oracle.steps(op, x, 1e-6, 50)
+        assert np.array_equal(a["states"], b["states"]) and np.array_equal(a["h"], b["h"])
