@@ -147,7 +147,7 @@ def _stream_ptr(stream):
 def get_derivatives(problem: SatProblem, x, out=None, logspace: bool = False, stream=None):
     """ISat::GetDerivatives for a [B, N+M] CUDA tensor of public states (float32 or
     float64).  float64 follows CpuSat<double> bit for bit; float32 with logspace=True
-    treats the a-block as ln a and returns d(ln a)/dt = K^2."""
+    treats the a-block as log2 a and returns d(log2 a)/dt = K^2 / ln 2."""
     import torch
     if not x.is_cuda:
         raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "get_derivatives needs a CUDA tensor")

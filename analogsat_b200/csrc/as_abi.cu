@@ -53,38 +53,46 @@ struct DevBuf {
 // Device copy of one or more packed instances in a single pool.
 struct DevicePool {
     int device = -1;
-    DevBuf lit, sell_row, sell, inst;
+    DevBuf lit, srow, perm, iperm, inst;
     std::vector<DevInstance> host_inst;
 
+    template <typename V>
+    static int put(const DevBuf& buf, size_t off, const V& v) {
+        if (!v.empty())
+            AS_CUDA(cudaMemcpy(static_cast<char*>(buf.p) + off * 4, v.data(), v.size() * 4,
+                               cudaMemcpyHostToDevice));
+        return AS_OK;
+    }
+
     int upload(const std::vector<const PackedProblem*>& pk, int dev) {
-        size_t nl = 0, nr = 0, ns = 0;
+        size_t nl = 0, nr = 0, np = 0;
         for (auto* q : pk) {
             nl += q->lit.size();
-            nr += q->sell_row.size();
-            ns += q->sell.size();
+            nr += q->srow.size();
+            np += q->perm.size();
         }
         AS_CUDA(lit.alloc(std::max<size_t>(nl, 1) * 4));
-        AS_CUDA(sell_row.alloc(std::max<size_t>(nr, 1) * 4));
-        AS_CUDA(sell.alloc(std::max<size_t>(ns, 1) * 4));
+        AS_CUDA(srow.alloc(std::max<size_t>(nr, 1) * 4));
+        AS_CUDA(perm.alloc(std::max<size_t>(np, 1) * 4));
+        AS_CUDA(iperm.alloc(std::max<size_t>(np, 1) * 4));
         AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
         host_inst.clear();
-        size_t ol = 0, orr = 0, os = 0;
+        size_t ol = 0, orr = 0, op = 0;
         for (auto* q : pk) {
             DevInstance d;
-            d.n = q->n; d.m = q->m; d.k = q->k; d.mp = q->mp; d.nslices = q->nslices; d.pad = 0;
+            d.n = q->n; d.m = q->m; d.k = q->k; d.mp = q->mp; d.nslices = q->nslices;
+            d.nslots = q->nslots;
             d.lit = lit.as<uint32_t>() + ol;
-            d.sell_row = sell_row.as<int32_t>() + orr;
-            d.sell = sell.as<int32_t>() + os;
-            if (!q->lit.empty())
-                AS_CUDA(cudaMemcpy((void*)d.lit, q->lit.data(), q->lit.size() * 4, cudaMemcpyHostToDevice));
-            if (!q->sell_row.empty())
-                AS_CUDA(cudaMemcpy((void*)d.sell_row, q->sell_row.data(), q->sell_row.size() * 4,
-                                   cudaMemcpyHostToDevice));
-            if (!q->sell.empty())
-                AS_CUDA(cudaMemcpy((void*)d.sell, q->sell.data(), q->sell.size() * 4, cudaMemcpyHostToDevice));
+            d.srow = srow.as<int32_t>() + orr;
+            d.perm = perm.as<int32_t>() + op;
+            d.iperm = iperm.as<int32_t>() + op;
+            int r;
+            if ((r = put(lit, ol, q->lit)) || (r = put(srow, orr, q->srow)) || (r = put(perm, op, q->perm)) ||
+                (r = put(iperm, op, q->iperm)))
+                return r;
             ol += q->lit.size();
-            orr += q->sell_row.size();
-            os += q->sell.size();
+            orr += q->srow.size();
+            op += q->perm.size();
             host_inst.push_back(d);
         }
         AS_CUDA(cudaMemcpy(inst.p, host_inst.data(), sizeof(DevInstance) * host_inst.size(),
@@ -131,11 +139,11 @@ const std::vector<Variant>& variants() {
 }
 
 size_t solver_smem(const Variant& v, const PackedProblem& q) {
-    return solve_smem_values<float>(q.n, q.m, q.k, q.mp) * v.bytes_per_value;
+    return solve_smem_values(q.n, q.m, q.nslots) * v.bytes_per_value;
 }
 
 bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_limit) {
-    return v.precision == precision && q.k <= v.kmax && solver_smem(v, q) <= smem_limit;
+    return q.compact && v.precision == precision && q.k <= v.kmax && solver_smem(v, q) <= smem_limit;
 }
 
 // Default CTA size: about four clauses per thread, 128..1024 threads.
@@ -289,6 +297,9 @@ namespace {
 
 int ensure_uploaded(as_problem* p) {
     if (p->host.m == 0 || p->host.k == 0) return fail(AS_ERR_NO_PROBLEM, "SAT problem has not been set");
+    if (!p->packed.compact)
+        return fail(AS_ERR_UNSUPPORTED, "instance too large for the shared-memory kernels "
+                                        "(needs N < 32768 and < 65535 contribution slots)");
     int dev = 0;
     AS_CUDA(cudaGetDevice(&dev));
     if (p->dev.device == dev) return AS_OK;
@@ -300,7 +311,7 @@ template <typename T, bool LOGA, int KMAX>
 int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
     constexpr int BT = 512;
     const auto& q = p->packed;
-    const size_t smem = ((size_t)((q.n + 1 + 3) & ~3) + (size_t)q.k * q.mp) * sizeof(T);
+    const size_t smem = rhs_smem_values(q.n, q.nslots) * sizeof(T);
     auto fn = &rhs_batch_kernel<T, LOGA, KMAX, BT>;
     int dev = 0, sms = 0, optin = 0, occ = 0;
     AS_CUDA(cudaGetDevice(&dev));

@@ -3,18 +3,18 @@
 // The ODE (AnalogSAT/cpu_sat/CpuSat.cpp:199-241, cpu_helper.h:101-126):
 //   K_m    = 2^-K prod_q (1 - c_mq s_q)            (K = max clause length)
 //   ds_i   = sum_m 2 a_m c_mi K_mi K_m,  K_mi = 2^-K prod_{q != i} (1 - c_mq s_q)
-//   da_m   = a_m K_m^2        (log space: du_m = K_m^2 with u_m = ln a_m)
+//   da_m   = a_m K_m^2   (FP32 path: a_m is held as u_m = log2 a_m, du_m = K_m^2 / ln 2)
 //
 // One RHS evaluation is two block-wide phases over shared memory:
 //   clause phase  thread-per-clause: gather K spins from `sy`, form K_m and the
-//                 leave-one-out products in registers, write each literal's
-//                 contribution 2 c K_mi K_m a_m to `contrib[q*mp + m]`
-//                 (coalesced, conflict-free) and return da_m;
-//   var phase     thread-per-variable: walk the variable's SELL-32 row list
-//                 (coalesced loads) and sum its contributions in clause order.
+//                 leave-one-out products in registers, store each literal's
+//                 contribution 2 c K_mi K_m a_m straight into its variable's slot of
+//                 the SELL-32 contribution buffer `cs`, return da_m;
+//   var phase     thread-per-variable: sum the variable's row of `cs` (contiguous,
+//                 bank-conflict free, no index loads) in clause order.
 // No atomics anywhere, so results are deterministic; in FP64 every operation is
 // an explicitly rounded mul/add in the reference's order, which makes the RHS
-// bit-identical to CpuSat<double>.
+// bit-identical to CpuSat<double>.  Layouts are documented in as_problem.h.
 #pragma once
 
 #include <cstdint>
@@ -22,13 +22,16 @@
 
 namespace asb {
 
-// One packed instance in device memory (layout documented in as_problem.h).
+// One packed instance in device memory.
 struct DevInstance {
-    int n, m, k, mp, nslices, pad;
-    const uint32_t* lit;
-    const int32_t* sell_row;
-    const int32_t* sell;
+    int n, m, k, mp, nslices, nslots;
+    const uint32_t* lit;   // [k][mp] literal words (var | sign | slot)
+    const int32_t* srow;   // [nslices + 1] SELL row offsets
+    const int32_t* perm;   // internal -> public variable
+    const int32_t* iperm;  // public -> internal variable
 };
+
+constexpr float kInvLn2 = 1.4426950408889634f;  // d(log2 a)/dt = (da/dt) / (a ln 2)
 
 // ---- explicitly rounded arithmetic: FP64 follows the reference bit for bit ----
 template <typename T> struct Arith;
@@ -36,22 +39,26 @@ template <> struct Arith<double> {
     static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
     static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
-    static __device__ __forceinline__ double ex(double u) { return exp(u); }
-    static __device__ __forceinline__ double lg(double a) { return log(a); }
 };
 template <> struct Arith<float> {
     static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
     static __device__ __forceinline__ float add(float a, float b) { return a + b; }
     static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
-    static __device__ __forceinline__ float ex(float u) { return expf(u); }
-    static __device__ __forceinline__ float lg(float a) { return logf(a); }
 };
 
-__device__ __forceinline__ uint32_t lit_var(uint32_t w) { return w & 0x7fffffffu; }
+// 2^u with the SFU (relative error ~2^-22, below the FP32 state's own rounding)
+__device__ __forceinline__ float exp2_fast(float u) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(u));
+    return r;
+}
 
-// Read-only loads of instance data that the compiler must not hoist out of the RK
-// stage loop (keeping them live across stages would cost registers, not traffic:
-// they hit L1).
+__device__ __forceinline__ uint32_t lit_var(uint32_t w) { return (w >> 16) & 0x7fffu; }
+__device__ __forceinline__ uint32_t lit_slot(uint32_t w) { return w & 0xffffu; }
+__device__ __forceinline__ bool lit_neg(uint32_t w) { return (w >> 31) != 0; }
+
+// Read-only loads of instance data, kept inside the stage loop (hoisting them would
+// cost registers across all six stages; they hit L1).
 __device__ __forceinline__ uint32_t ld_ro(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.global.nc.L1::evict_last.u32 %0, [%1];" : "=r"(v) : "l"(p));
@@ -62,16 +69,15 @@ __device__ __forceinline__ int32_t ld_ro(const int32_t* p) {
     asm volatile("ld.global.nc.L1::evict_last.s32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
 }
-__device__ __forceinline__ bool lit_neg(uint32_t w) { return (w >> 31) != 0; }
 
-// Clause phase for one clause m: returns da_m (or du_m in log space), writes the
-// per-literal spin contributions into contrib.  `am` is a_m in linear space.
-// KMAX bounds the runtime clause length k.  For k <= 10 the leave-one-out
-// products follow CpuProdWrapper (ascending, left-associated); for k > 10 the
-// generic CalculateAll form (CpuSat.cpp:291-349) is used.
+// Clause phase for one clause m: stores the per-literal spin contributions into cs
+// and returns da_m (du_m in log space).  `am` is a_m in linear space.  KMAX bounds
+// the runtime clause length k.  For k <= 10 the leave-one-out products follow
+// CpuProdWrapper (ascending, left-associated); for k > 10 the generic CalculateAll
+// form (CpuSat.cpp:291-349).
 template <typename T, bool LOGA, int KMAX>
 __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* __restrict__ sy,
-                                          T* __restrict__ contrib, T am, T knorm) {
+                                          T* __restrict__ cs, T am, T knorm) {
     using A = Arith<T>;
     uint32_t w[KMAX];
     T f[KMAX];
@@ -79,18 +85,20 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
 #pragma unroll
     for (int q = 0; q < KMAX; q++) {
         if (q < I.k) {
-            w[q] = ld_ro(I.lit + (size_t)q * I.mp + m);
+            w[q] = ld_ro(I.lit + q * I.mp + m);
             const T s = sy[lit_var(w[q])];
             f[q] = lit_neg(w[q]) ? A::add(T(1), s) : A::sub(T(1), s);
             km = A::mul(km, f[q]);
         }
     }
-    const T dam = LOGA ? A::mul(km, km) : A::mul(A::mul(am, km), km);
+    T dam;
+    if constexpr (LOGA) dam = km * km * T(kInvLn2);
+    else dam = A::mul(A::mul(am, km), km);
     if (KMAX <= 10 || I.k <= 10) {
         const T r = A::mul(A::mul(km, knorm), am);
 #pragma unroll
         for (int q = 0; q < KMAX; q++) {
-            if (q < I.k && lit_var(w[q]) != (uint32_t)I.n) {
+            if (q < I.k && lit_slot(w[q]) != 0xffffu) {
                 T prod = T(1);
                 bool first = true;
 #pragma unroll
@@ -101,65 +109,49 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
                     }
                 }
                 T rr = A::mul(r, prod);
-                rr = lit_neg(w[q]) ? -(rr + rr) : (rr + rr);
-                contrib[q * I.mp + m] = rr;
+                rr = rr + rr;
+                cs[lit_slot(w[q])] = lit_neg(w[q]) ? -rr : rr;
             }
         }
     } else {
 #pragma unroll
         for (int q = 0; q < KMAX; q++) {
-            if (q < I.k && lit_var(w[q]) != (uint32_t)I.n) {
+            if (q < I.k && lit_slot(w[q]) != 0xffffu) {
                 T temp = km;
 #pragma unroll
                 for (int l = 0; l < KMAX; l++)
                     if (l < I.k) temp = A::mul(temp, l == q ? T(1) : f[l]);
-                T rr = A::mul(A::mul(A::mul(T(2), temp), knorm), am);
-                contrib[q * I.mp + m] = lit_neg(w[q]) ? -rr : rr;
+                const T rr = A::mul(A::mul(A::mul(T(2), temp), knorm), am);
+                cs[lit_slot(w[q])] = lit_neg(w[q]) ? -rr : rr;
             }
         }
     }
     return dam;
 }
 
-// Var phase for variable i (< n): sum of its contributions in (clause, slot) order.
+// Var phase for internal variable v (< n): sum of its SELL row in clause order.
+// Padding slots are zero (x + 0 == x, and the reference's sums are never -0).
 template <typename T>
-__device__ __forceinline__ T var_phase(const DevInstance& I, int i, const T* __restrict__ contrib) {
+__device__ __forceinline__ T var_phase(const DevInstance& I, int v, const T* __restrict__ cs) {
     using A = Arith<T>;
-    const int g = i >> 5, lane = i & 31;
-    const int r0 = ld_ro(I.sell_row + g), r1 = ld_ro(I.sell_row + g + 1);
+    const int g = v >> 5;
+    const int r0 = ld_ro(I.srow + g), r1 = ld_ro(I.srow + g + 1);
+    const T* p = cs + r0 * 32 + (v & 31);
     T sum = T(0);
-    for (int r = r0; r < r1; r++) {
-        const int e = ld_ro(I.sell + (size_t)r * 32 + lane);
-        if (e < 0) break;
-        sum = A::add(sum, contrib[e]);
-    }
+    for (int r = r0; r < r1; r++, p += 32) sum = A::add(sum, *p);
     return sum;
 }
 
 // Clause check for clause m against the spins in sy (CpuSat.cpp:136-164): a
 // variable is TRUE when s > 0; the sentinel (s = -1, positive) is FALSE.
-template <int KMAX>
-__device__ __forceinline__ int clause_violated(const DevInstance& I, int m, const float* sy) {
+template <int KMAX, typename T>
+__device__ __forceinline__ int clause_violated(const DevInstance& I, int m, const T* sy) {
     bool sat = false;
 #pragma unroll
     for (int q = 0; q < KMAX; q++) {
         if (q < I.k) {
-            const uint32_t w = __ldg(I.lit + (size_t)q * I.mp + m);
-            const bool t = sy[lit_var(w)] > 0.0f;
-            sat |= lit_neg(w) ? !t : t;
-        }
-    }
-    return sat ? 0 : 1;
-}
-
-template <int KMAX>
-__device__ __forceinline__ int clause_violated(const DevInstance& I, int m, const double* sy) {
-    bool sat = false;
-#pragma unroll
-    for (int q = 0; q < KMAX; q++) {
-        if (q < I.k) {
-            const uint32_t w = __ldg(I.lit + (size_t)q * I.mp + m);
-            const bool t = sy[lit_var(w)] > 0.0;
+            const uint32_t w = ld_ro(I.lit + q * I.mp + m);
+            const bool t = sy[lit_var(w)] > T(0);
             sat |= lit_neg(w) ? !t : t;
         }
     }
@@ -168,31 +160,37 @@ __device__ __forceinline__ int clause_violated(const DevInstance& I, int m, cons
 
 // ---- block reductions (warp shuffles + one smem slot per warp) ----
 template <int BT>
-__device__ __forceinline__ double block_max(double v, double* red) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __syncthreads();  // red may still be read from the previous reduction
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    v = red[0];
-#pragma unroll
-    for (int w = 1; w < BT / 32; w++) v = fmax(v, red[w]);
-    return v;
-}
-
-template <int BT>
 __device__ __forceinline__ int block_sum(int v, int* red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __syncthreads();
+    __syncthreads();  // red may still be read from the previous reduction
     if (lane == 0) red[warp] = v;
     __syncthreads();
     int s = 0;
 #pragma unroll
     for (int w = 0; w < BT / 32; w++) s += red[w];
     return s;
+}
+
+// Block max (FP64) whose result is post-processed by thread 0: fn(max) is broadcast
+// to every thread; fn may publish more values in red[BT/32 + 1 ...].
+template <int BT, typename F>
+__device__ __forceinline__ double block_max_then(double v, double* red, F&& fn) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();  // red may still be read from the previous reduction
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+#pragma unroll
+        for (int w = 1; w < BT / 32; w++) m = fmax(m, red[w]);
+        red[BT / 32] = fn(m);
+    }
+    __syncthreads();
+    return red[BT / 32];
 }
 
 }  // namespace asb

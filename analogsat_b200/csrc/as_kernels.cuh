@@ -105,29 +105,30 @@ __device__ __forceinline__ T rk_new(T x, T k1, T k3, T k4, T k6, T h) {
                                       A::mul(T(ck::c6), k6))));
 }
 
-// |xerr / xscal| in FP64 (the controller's error norm is always accumulated in FP64).
-// xscal = |x| + |k1 h0| + TINY (CpuRungeKutta.cpp:85); in log space the a-block uses
-// 1 + |k1 h0| + TINY, i.e. the reference's relative error of a.
-template <typename T>
-__device__ __forceinline__ double rk_err_ratio(T x, T k1, T k3, T k4, T k5, T k6, double h,
-                                               double h0, bool unit_scale) {
+// Error ratio |xerr / xscal| of one element (CpuRungeKutta.cpp:214, 233-235) with
+// xscal = |x| + |k1 h0| + TINY (CpuRungeKutta.cpp:85).
+// FP64 state: every operation rounded in the reference's order.
+// FP32 state: formed in FP32 -- the k_j carry FP32 rounding already, so wider
+// arithmetic here cannot sharpen the estimate; the max over elements and the
+// controller run in FP64.  For log-space clause weights (u = log2 a) the scale is
+// 1/ln2 + |k1 h0|: the reference's |a| + |h da/dt| expressed in u, i.e. the same
+// relative error of a.
+__device__ __forceinline__ double rk_err_ratio(double x, double k1, double k3, double k4, double k5,
+                                               double k6, double h, double h0, bool) {
     using D = Arith<double>;
     const double e = D::mul(
-        h, D::add(D::add(D::add(D::add(D::mul(ck::dc1, (double)k1), D::mul(ck::dc3, (double)k3)),
-                                D::mul(ck::dc4, (double)k4)),
-                         D::mul(ck::dc5, (double)k5)),
-                  D::mul(ck::dc6, (double)k6)));
-    const double xa = unit_scale ? 1.0 : fabs((double)x);
-    if constexpr (sizeof(T) == 8) {
-        const double sc = D::add(D::add(xa, fabs(D::mul((double)k1, h0))), ck::TINY);
-        return fabs(__ddiv_rn(e, sc));
-    } else {
-        // FP32 state: the cancellation-prone error sum and the scale are FP64; their
-        // quotient only feeds a tolerance test, so it is formed in FP32 (an IEEE FP64
-        // divide here costs more registers than the whole RHS).
-        const double sc = xa + fabs((double)(k1 * (T)h0)) + ck::TINY;
-        return (double)fabsf(__fdiv_rn((float)e, (float)sc));
-    }
+        h, D::add(D::add(D::add(D::add(D::mul(ck::dc1, k1), D::mul(ck::dc3, k3)), D::mul(ck::dc4, k4)),
+                         D::mul(ck::dc5, k5)),
+                  D::mul(ck::dc6, k6)));
+    const double sc = D::add(D::add(fabs(x), fabs(D::mul(k1, h0))), ck::TINY);
+    return fabs(__ddiv_rn(e, sc));
+}
+__device__ __forceinline__ float rk_err_ratio(float x, float k1, float k3, float k4, float k5,
+                                              float k6, float h, float h0, bool logw) {
+    const float e = h * (float(ck::dc1) * k1 + float(ck::dc3) * k3 + float(ck::dc4) * k4 +
+                         float(ck::dc5) * k5 + float(ck::dc6) * k6);
+    const float sc = (logw ? kInvLn2 : fabsf(x)) + fabsf(k1 * h0) + 1e-20f;
+    return __fdividef(fabsf(e), sc);
 }
 
 template <int BT>
@@ -140,46 +141,47 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 // ---------------------------------------------------------------------------
 // Persistent solver kernel
 // ---------------------------------------------------------------------------
-// Shared-memory layout of one trajectory (E = n + m state elements, public order:
-// spins 0..n-1, then clause weights n..n+m-1):
+// Shared-memory layout of one trajectory (E = n + m state elements: internal
+// variables 0..n-1, then clause weights n..n+m-1):
 //   X, K1..K5   the RK stage vectors (state, k1..k5), E values each;
 //   sy          the stage's spin vector plus the sentinel slot sy[n] = -1;
-//   contrib     per-literal spin contributions, k * mp values.
-// Element e is owned by thread e % BT in every loop, so stage vectors need no
-// barriers; only sy and contrib are exchanged between threads.
+//   cs          SELL-32 contribution slots (nslots values, padding kept at 0).
+// Element e is owned by thread e % BT in every stage loop, so stage vectors need no
+// barriers; only sy and cs are exchanged between threads.
 template <typename T>
 struct Stages {
     T *X, *K1, *K2, *K3, *K4, *K5;
 };
 
-template <typename T>
-__host__ __device__ inline size_t solve_smem_values(int n, int m, int k, int mp) {
+__host__ __device__ inline size_t solve_smem_values(int n, int m, int nslots) {
     const size_t E = (size_t)((n + m + 3) & ~3);
-    return 6 * E + (size_t)((n + 1 + 3) & ~3) + (size_t)k * mp;
+    return 6 * E + (size_t)((n + 1 + 3) & ~3) + (size_t)nslots;
 }
 
 template <typename T, bool LOGA, int KMAX, int BT>
 struct Solver {
     using A = Arith<T>;
+    using ET = T;  // error-ratio type (see rk_err_ratio)
 
     // One RHS evaluation at stage S.  The stage input is formed on the fly from the
     // stage vectors; the derivative lands in K_S, or for S == 6 is consumed at once
     // into xnew (stored in K2, dead after the stage-6 input) and the error norm.
     template <int S>
-    static __device__ __forceinline__ void eval(const DevInstance& I, T* sy, T* contrib, T knorm,
-                                                const Stages<T>& st, T hT, double h, double h0,
-                                                double& errmax) {
+    static __device__ __forceinline__ void eval(const DevInstance& I, T* sy, T* cs, T knorm,
+                                                const Stages<T>& st, T hT, T h0T, ET& errmax) {
         const int tid = threadIdx.x;
         const int n = I.n;
-        for (int i = tid; i < n; i += BT)
-            sy[i] = stage_in<S>(st.X[i], st.K1[i], st.K2[i], st.K3[i], st.K4[i], st.K5[i], hT);
+        for (int v = tid; v < n; v += BT)
+            sy[v] = stage_in<S>(st.X[v], st.K1[v], st.K2[v], st.K3[v], st.K4[v], st.K5[v], hT);
         __syncthreads();
         for (int m = tid; m < I.m; m += BT) {
             const int e = n + m;
             const T x = st.X[e];
             const T y = stage_in<S>(x, st.K1[e], st.K2[e], st.K3[e], st.K4[e], st.K5[e], hT);
-            const T am = LOGA ? A::ex(y) : y;
-            const T d = clause_phase<T, LOGA, KMAX>(I, m, sy, contrib, am, knorm);
+            T am;
+            if constexpr (LOGA) am = exp2_fast(y);
+            else am = y;
+            const T d = clause_phase<T, LOGA, KMAX>(I, m, sy, cs, am, knorm);
             if constexpr (S == 1) st.K1[e] = d;
             if constexpr (S == 2) st.K2[e] = d;
             if constexpr (S == 3) st.K3[e] = d;
@@ -187,22 +189,22 @@ struct Solver {
             if constexpr (S == 5) st.K5[e] = d;
             if constexpr (S == 6) {
                 const T k1 = st.K1[e], k3 = st.K3[e], k4 = st.K4[e];
-                errmax = fmax(errmax, rk_err_ratio<T>(x, k1, k3, k4, st.K5[e], d, h, h0, LOGA));
+                errmax = fmax(errmax, rk_err_ratio(x, k1, k3, k4, st.K5[e], d, hT, h0T, LOGA));
                 st.K2[e] = rk_new<T>(x, k1, k3, k4, d, hT);
             }
         }
         __syncthreads();
-        for (int i = tid; i < n; i += BT) {
-            const T d = var_phase<T>(I, i, contrib);
-            if constexpr (S == 1) st.K1[i] = d;
-            if constexpr (S == 2) st.K2[i] = d;
-            if constexpr (S == 3) st.K3[i] = d;
-            if constexpr (S == 4) st.K4[i] = d;
-            if constexpr (S == 5) st.K5[i] = d;
+        for (int v = tid; v < n; v += BT) {
+            const T d = var_phase<T>(I, v, cs);
+            if constexpr (S == 1) st.K1[v] = d;
+            if constexpr (S == 2) st.K2[v] = d;
+            if constexpr (S == 3) st.K3[v] = d;
+            if constexpr (S == 4) st.K4[v] = d;
+            if constexpr (S == 5) st.K5[v] = d;
             if constexpr (S == 6) {
-                const T x = st.X[i], k1 = st.K1[i], k3 = st.K3[i], k4 = st.K4[i];
-                errmax = fmax(errmax, rk_err_ratio<T>(x, k1, k3, k4, st.K5[i], d, h, h0, false));
-                st.K2[i] = rk_new<T>(x, k1, k3, k4, d, hT);
+                const T x = st.X[v], k1 = st.K1[v], k3 = st.K3[v], k4 = st.K4[v];
+                errmax = fmax(errmax, rk_err_ratio(x, k1, k3, k4, st.K5[v], d, hT, h0T, false));
+                st.K2[v] = rk_new<T>(x, k1, k3, k4, d, hT);
             }
         }
     }
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
     using A = Arith<T>;
     using S = Solver<T, LOGA, KMAX, BT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[BT / 32];
+    __shared__ double red_d[BT / 32 + 2];
     __shared__ int red_i[BT / 32];
     __shared__ int s_unit, s_flag;
     const int tid = threadIdx.x;
@@ -230,16 +232,18 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
         T* base = reinterpret_cast<T*>(smem_raw);
         Stages<T> st{base, base + Ep, base + 2 * Ep, base + 3 * Ep, base + 4 * Ep, base + 5 * Ep};
         T* sy = base + 6 * Ep;
-        T* contrib = sy + ((n + 1 + 3) & ~3);
+        T* cs = sy + ((n + 1 + 3) & ~3);
         T* G = reinterpret_cast<T*>(P.states) + P.unit_state[u];
         const T knorm = (T)ldexp(1.0, -I.k);
 
-        // load the initial state (a -> ln a in log space)
-        for (int e = tid; e < E; e += BT) {
-            const T v = G[e];
-            st.X[e] = (LOGA && e >= n) ? A::lg(v) : v;
-            st.K1[e] = st.K2[e] = st.K3[e] = st.K4[e] = st.K5[e] = T(0);
+        // initial state: public spins scattered to internal order; a -> log2 a
+        for (int i = tid; i < n; i += BT) st.X[__ldg(I.iperm + i)] = G[i];
+        for (int e = n + tid; e < E; e += BT) {
+            const T a = G[e];
+            if constexpr (LOGA) st.X[e] = log2f(a);
+            else st.X[e] = a;
         }
+        for (int j = tid; j < I.nslots; j += BT) cs[j] = T(0);
         if (tid == 0) sy[n] = T(-1);  // sentinel spin: padding literals are always FALSE
 
         double t = 0.0, hnext = 1e-9, hdid = 0.0;
@@ -256,30 +260,42 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
             int taken = 0;
             for (int b = 0; b < P.batch; b++) {
                 // ---- CpuRungeKutta::Step, count = 1 ----
-                double dummy = 0.0;
-                S::template eval<1>(I, sy, contrib, knorm, st, T(0), 0.0, 0.0, dummy);
+                T dummy = T(0);
+                S::template eval<1>(I, sy, cs, knorm, st, T(0), T(0), dummy);
                 rhs++;
                 const double h0 = hnext;
+                const T h0T = (T)h0;
                 double h = hnext, ermax = 0.0;
                 while (true) {
                     const T hT = (T)h;
-                    double em = 0.0;
-                    S::template eval<2>(I, sy, contrib, knorm, st, hT, h, h0, em);
-                    S::template eval<3>(I, sy, contrib, knorm, st, hT, h, h0, em);
-                    S::template eval<4>(I, sy, contrib, knorm, st, hT, h, h0, em);
-                    S::template eval<5>(I, sy, contrib, knorm, st, hT, h, h0, em);
-                    S::template eval<6>(I, sy, contrib, knorm, st, hT, h, h0, em);
+                    T em = T(0);
+                    S::template eval<2>(I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<3>(I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<4>(I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<5>(I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<6>(I, sy, cs, knorm, st, hT, h0T, em);
                     rhs += 5;
                     attempts++;
-                    ermax = __ddiv_rn(block_max<BT>(em, red_d), P.eps);
-                    if (ermax <= 1.0) break;
-                    const double htemp = __dmul_rn(__dmul_rn(ck::SAFETY, h), pow(ermax, ck::PSHRNK));
-                    h = fmax(htemp, __dmul_rn(ck::HFACTOR, h));
+                    // step-size control (CpuRungeKutta.cpp:229-259): one thread evaluates
+                    // pow() and broadcasts the new step size with the error norm
+                    ermax = block_max_then<BT>((double)em, red_d, [&](double emax) {
+                        const double e = __ddiv_rn(emax, P.eps);
+                        double hn;
+                        if (e <= 1.0)
+                            hn = e > ck::ERRCON ? __dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PGROW))
+                                                : __dmul_rn(5.0, h);
+                        else
+                            hn = fmax(__dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PSHRNK)),
+                                      __dmul_rn(ck::HFACTOR, h));
+                        red_d[BT / 32 + 1] = hn;
+                        return e;
+                    });
+                    const double hn = red_d[BT / 32 + 1];
+                    if (ermax <= 1.0) { hnext = hn; break; }
+                    h = hn;
                     if (__dadd_rn(t, h) == t) { underflow = true; break; }
                 }
                 if (underflow) break;
-                hnext = ermax > ck::ERRCON ? __dmul_rn(__dmul_rn(ck::SAFETY, h), pow(ermax, ck::PGROW))
-                                           : __dmul_rn(5.0, h);
                 hdid = h;
                 t = __dadd_rn(t, h);
                 taken++;
@@ -290,7 +306,7 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
             steps += taken;
 
             // ---- CpuSat::GetClauseViolationCount on the accepted state ----
-            for (int i = tid; i < n; i += BT) sy[i] = st.X[i];
+            for (int v = tid; v < n; v += BT) sy[v] = st.X[v];
             __syncthreads();
             int cnt = 0;
             for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX>(I, m, sy);
@@ -301,7 +317,8 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
                     uint32_t* bits = P.best_bits + P.unit_bits[u];
                     for (int i0 = tid & ~31; i0 < n; i0 += BT) {
                         const int i = i0 + (tid & 31);
-                        const unsigned bal = __ballot_sync(0xffffffffu, i < n && sy[i < n ? i : 0] > T(0));
+                        const bool b = i < n && sy[__ldg(I.iperm + (i < n ? i : 0))] > T(0);
+                        const unsigned bal = __ballot_sync(0xffffffffu, b);
                         if ((tid & 31) == 0) bits[i0 >> 5] = bal;
                     }
                 }
@@ -326,9 +343,12 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
         }
 
         // write back the final state in the public layout
-        for (int e = tid; e < E; e += BT) {
+        __syncthreads();
+        for (int i = tid; i < n; i += BT) G[i] = st.X[__ldg(I.iperm + i)];
+        for (int e = n + tid; e < E; e += BT) {
             const T v = st.X[e];
-            G[e] = (LOGA && e >= n) ? A::ex(v) : v;
+            if constexpr (LOGA) G[e] = exp2f(v);
+            else G[e] = v;
         }
         if (tid == 0) {
             UnitResult r;
@@ -342,29 +362,43 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
 }
 
 // ---------------------------------------------------------------------------
-// Standalone batched RHS: one CTA per trajectory, state in global memory.
+// Standalone batched RHS: one CTA per state, states in global memory (public
+// layout).  Reads of x and writes of dxdt are coalesced; the permutation to the
+// internal variable order happens in shared memory.
 // ---------------------------------------------------------------------------
+__host__ __device__ inline size_t rhs_smem_values(int n, int nslots) {
+    return (size_t)((n + 1 + 3) & ~3) + (size_t)nslots;
+}
+
 template <typename T, bool LOGA, int KMAX, int BT>
 __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* __restrict__ x,
                                                         T* __restrict__ dxdt, int ntraj,
                                                         long long stride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sy = reinterpret_cast<T*>(smem_raw);
-    T* contrib = sy + ((I.n + 1 + 3) & ~3);
+    T* cs = sy + ((I.n + 1 + 3) & ~3);
     const int tid = threadIdx.x;
+    const int n = I.n;
     const T knorm = (T)ldexp(1.0, -I.k);
+    for (int j = tid; j < I.nslots; j += BT) cs[j] = T(0);
     for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
         const T* X = x + (long long)tr * stride;
         T* D = dxdt + (long long)tr * stride;
-        for (int i = tid; i < I.n; i += BT) sy[i] = X[i];
-        if (tid == 0) sy[I.n] = T(-1);
+        for (int i = tid; i < n; i += BT) sy[__ldg(I.iperm + i)] = X[i];
+        if (tid == 0) sy[n] = T(-1);
         __syncthreads();
         for (int m = tid; m < I.m; m += BT) {
-            const T a = X[I.n + m];
-            D[I.n + m] = clause_phase<T, LOGA, KMAX>(I, m, sy, contrib, LOGA ? Arith<T>::ex(a) : a, knorm);
+            const T a = X[n + m];
+            T am;
+            if constexpr (LOGA) am = exp2_fast(a);
+            else am = a;
+            D[n + m] = clause_phase<T, LOGA, KMAX>(I, m, sy, cs, am, knorm);
         }
         __syncthreads();
-        for (int i = tid; i < I.n; i += BT) D[i] = var_phase<T>(I, i, contrib);
+        // ds in internal order -> sy (no longer read) -> public order, coalesced
+        for (int v = tid; v < n; v += BT) sy[v] = var_phase<T>(I, v, cs);
+        __syncthreads();
+        for (int i = tid; i < n; i += BT) D[i] = sy[__ldg(I.iperm + i)];
         __syncthreads();
     }
 }
@@ -380,7 +414,7 @@ __global__ void __launch_bounds__(BT) viol_batch_kernel(DevInstance I, const T* 
     const int tid = threadIdx.x;
     for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
         const T* X = x + (long long)tr * stride;
-        for (int i = tid; i < I.n; i += BT) sy[i] = X[i];
+        for (int i = tid; i < I.n; i += BT) sy[__ldg(I.iperm + i)] = X[i];
         if (tid == 0) sy[I.n] = T(-1);
         __syncthreads();
         int cnt = 0;

@@ -96,45 +96,43 @@ PackedProblem pack(const HostProblem& p) {
     q.k = p.k;
     q.mp = std::max(32, (p.m + 31) / 32 * 32);
     q.nslices = (p.n + 31) / 32;
-    const uint32_t sentinel = (uint32_t)p.n;
-    q.lit.assign((size_t)q.k * q.mp, sentinel);
 
-    // incidence lists per variable, in (clause, slot) order
+    // degree of every public variable and its incidences in (clause, slot) order
     std::vector<int32_t> degree(p.n, 0);
     for (int j = 0; j < p.m; j++)
         for (int i = 0; i < p.length[j]; i++) degree[std::abs(p.storage[p.start[j] + i]) - 1]++;
-    std::vector<int64_t> off(p.n + 1, 0);
-    for (int v = 0; v < p.n; v++) off[v + 1] = off[v] + degree[v];
-    std::vector<int32_t> inc((size_t)off[p.n]);
-    std::vector<int64_t> fill(off.begin(), off.end() - 1);
-    for (int j = 0; j < p.m; j++) {
-        for (int i = 0; i < p.length[j]; i++) {
-            const int lit = p.storage[p.start[j] + i];
-            const int v = std::abs(lit) - 1;
-            q.lit[(size_t)i * q.mp + j] = (uint32_t)v | (lit < 0 ? 0x80000000u : 0u);
-            inc[fill[v]++] = i * q.mp + j;
-        }
-    }
     q.max_degree = 0;
     for (int v = 0; v < p.n; v++) q.max_degree = std::max(q.max_degree, degree[v]);
 
-    // SELL-32 slices
-    q.sell_row.assign(q.nslices + 1, 0);
+    // internal order: decreasing degree, ties by public index
+    q.perm.resize(p.n);
+    for (int v = 0; v < p.n; v++) q.perm[v] = v;
+    std::stable_sort(q.perm.begin(), q.perm.end(),
+                     [&](int a, int b) { return degree[a] > degree[b]; });
+    q.iperm.resize(p.n);
+    for (int v = 0; v < p.n; v++) q.iperm[q.perm[v]] = v;
+
+    // SELL-32 rows: slice g is as wide as its largest degree
+    q.srow.assign(q.nslices + 1, 0);
     for (int g = 0; g < q.nslices; g++) {
         int w = 0;
-        for (int l = 0; l < 32; l++) {
-            const int v = g * 32 + l;
-            if (v < p.n) w = std::max(w, degree[v]);
-        }
-        q.sell_row[g + 1] = q.sell_row[g] + w;
+        for (int l = 0; l < 32 && g * 32 + l < p.n; l++) w = std::max(w, degree[q.perm[g * 32 + l]]);
+        q.srow[g + 1] = q.srow[g] + w;
     }
-    q.sell.assign((size_t)q.sell_row[q.nslices] * 32, -1);
-    for (int g = 0; g < q.nslices; g++) {
-        for (int l = 0; l < 32; l++) {
-            const int v = g * 32 + l;
-            if (v >= p.n) continue;
-            for (int r = 0; r < degree[v]; r++)
-                q.sell[((size_t)q.sell_row[g] + r) * 32 + l] = inc[off[v] + r];
+    q.nslots = q.srow[q.nslices] * 32;
+    q.compact = p.n < 32768 && q.nslots < (int)kPadSlot;
+
+    const uint32_t pad = ((uint32_t)std::min(p.n, 32767) << 16) | kPadSlot;
+    q.lit.assign((size_t)q.k * q.mp, pad);
+    std::vector<int32_t> rank(p.n, 0);  // next row of each internal variable
+    for (int j = 0; j < p.m; j++) {
+        for (int i = 0; i < p.length[j]; i++) {
+            const int lit = p.storage[p.start[j] + i];
+            const int v = q.iperm[std::abs(lit) - 1];
+            const int slot = (q.srow[v >> 5] + rank[v]++) * 32 + (v & 31);
+            if (q.compact)
+                q.lit[(size_t)i * q.mp + j] =
+                    (lit < 0 ? 0x80000000u : 0u) | ((uint32_t)v << 16) | (uint32_t)slot;
         }
     }
     return q;

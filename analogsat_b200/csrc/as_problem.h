@@ -5,21 +5,27 @@
 // filtered, empty clauses are dropped, N = max |literal| and K = max clause length
 // (SatProblem.cpp:38-95).
 //
-// PackedProblem is the device layout of one instance:
-//   lit[q * mp + m]   packed literal word of clause m, slot q (q < k, m < mp):
-//                     bits 0..30 = 0-based variable index, bit 31 = negated.
-//                     Slots past a clause's length hold the sentinel variable N,
-//                     whose spin is held at -1, so each contributes the factor 2
-//                     exactly like the reference's zero padding against its
-//                     constant FALSE slot (AnalogSAT/cpu_sat/CpuSat.cpp:214-215).
-//   sell              var -> (clause, slot) incidence as SELL-32: variables are
-//                     cut into slices of 32; slice g owns rows
-//                     [sell_row[g], sell_row[g+1]) of 32 entries, lane l of row r
-//                     is the r-th incidence of variable 32g+l, given as the
-//                     contribution index q * mp + m, -1 past its degree.  Rows
-//                     of a variable are ordered by (clause, slot), which is the
-//                     order the reference accumulates ds_i in (CpuSat.cpp:203-236),
-//                     so FP64 sums are bit-identical.
+// PackedProblem is the device layout of one instance.
+//  * Variables are renumbered internally by decreasing degree (number of clause
+//    occurrences): perm[v] = public 0-based index of internal variable v, iperm is
+//    its inverse.  Groups of 32 consecutive internal variables ("slices") then have
+//    nearly equal degrees, so the SELL layout below carries little padding.
+//  * Contribution slots (SELL-32): slice g owns rows [srow[g], srow[g+1]) of 32
+//    slots; slot (row r, lane l) holds the r-th clause contribution to internal
+//    variable 32g+l, rows ordered by (clause, slot) -- the order in which the
+//    reference accumulates ds_i (AnalogSAT/cpu_sat/CpuSat.cpp:203-236), so FP64 sums
+//    are bit-identical.  Slots past a variable's degree stay 0.
+//  * Literal words lit[q * mp + m] (clause m, slot q < k, clause stride mp = M
+//    rounded up to 32), one uint32 each:
+//        bit 31     negated literal
+//        bits 16-30 internal variable index
+//        bits 0-15  contribution slot of this literal
+//    Slots past a clause's length hold the sentinel word (var = N, slot 0xffff):
+//    the sentinel spin is held at -1, so each contributes the factor 2 exactly like
+//    the reference's zero padding against its constant FALSE slot
+//    (CpuSat.cpp:214-215), and its contribution is dropped.
+//    This "compact" encoding needs N < 32768 and fewer than 65535 slots; larger
+//    instances are rejected by the shared-memory kernels.
 #pragma once
 
 #include <cstdint>
@@ -43,13 +49,18 @@ bool read_cnf(const char* path, HostProblem& p, std::string& msg);
 // CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74).
 bool write_cnf(const char* path, const HostProblem& p);
 
+constexpr uint32_t kPadSlot = 0xffffu;
+
 struct PackedProblem {
     int n = 0, m = 0, k = 0;
-    int mp = 0;         // clause stride: m rounded up to a multiple of 32
-    int nslices = 0;    // ceil(n / 32)
-    std::vector<uint32_t> lit;       // [k][mp]
-    std::vector<int32_t> sell_row;   // [nslices + 1]
-    std::vector<int32_t> sell;       // [sell_row[nslices]][32]
+    int mp = 0;          // clause stride: m rounded up to a multiple of 32
+    int nslices = 0;     // ceil(n / 32)
+    int nslots = 0;      // srow[nslices] * 32
+    bool compact = false;
+    std::vector<uint32_t> lit;     // [k][mp] literal words
+    std::vector<int32_t> srow;     // [nslices + 1]
+    std::vector<int32_t> perm;     // internal -> public variable
+    std::vector<int32_t> iperm;    // public -> internal variable
     int max_degree = 0;
 };
 

@@ -11,9 +11,13 @@ runs all 16,384 trajectories to their SatResult in one persistent launch.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Metric: solves/s = trajectories that reached SAT_SOLUTION_FOUND per second (every
-solution verified by the exact clause check); RHS evaluations/s and instances/s
-(instances with >= 1 solved trajectory) are reported beside it.  `value` is timed
+Metric: solves/s = instances solved per second.  The 256 trajectories of an instance
+race from independent random starts and the first solution stops the others
+(early exit on device); every reported solution passes the exact clause check.  The
+reference's plain method solves an instance with one trajectory per Solve() call,
+so its solves/s is Solve() calls that found a solution per second.  RHS
+evaluations/s and trajectory-level counts are reported beside it
+(--all-trajectories runs every trajectory to its own SatResult instead).  `value` is timed
 with CUDA events with the initial states already in HBM; `e2e` goes through the
 C ABI from pinned host buffers (H2D of the initial states, D2H of the results and
 final states inside the timed region).
@@ -56,6 +60,11 @@ def parse_args():
     ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-rhs-bench", action="store_true")
+    ap.add_argument("--all-trajectories", action="store_true",
+                    help="run every trajectory to its own SatResult (no early exit per instance)")
+    ap.add_argument("--max-steps", type=int, default=WORKLOAD["maxsteps"],
+                    help="per-trajectory step cap (profiling runs use a small one)")
     return ap.parse_args()
 
 
@@ -137,9 +146,10 @@ def cpu_baseline(probs, pidx, ics, seconds: float, nthreads=None):
     handles = [rp[i] for i in used]
     remap = {i: k for k, i in enumerate(used)}
     nm = W["n"] + W["m"]
+    ics = ics.reshape(-1, nm)
     sample = order[:4096]
     units_p = np.array([remap[pidx[u]] for u in sample], np.int32)
-    units_x = [ics[u * nm:(u + 1) * nm].astype(np.float64) for u in sample]
+    units_x = [ics[u].astype(np.float64) for u in sample]
     r = R.solve_many(handles, units_p, units_x, eps=W["eps"], tmax=W["tmax"],
                      maxsteps=W["maxsteps"], batch=W["batch"], nthreads=nthreads,
                      wall_budget=seconds)
@@ -213,8 +223,9 @@ def run_ours(args):
     solver = A.SatSolver(probs, precision=A.AS_PREC_F32_LOGA, device=local)
     solver.SetEpsilon(W["eps"])
     solver.SetBatchSize(W["batch"])
-    solver.SetMaxSteps(W["maxsteps"])
+    solver.SetMaxSteps(args.max_steps)
     solver.SetMaxTime(W["tmax"])
+    solver.SetStopOnFirst(not args.all_trajectories)
     ics_dev = torch.from_numpy(ics).cuda()
     st = torch.cuda.Stream()
     nm = W["n"] + W["m"]
@@ -242,7 +253,7 @@ def run_ours(args):
     verify_solutions(solver, probs_raw, pidx, r, nm)
 
     barrier()
-    totals = dict(solved=0, rhs=0, inst=0)
+    totals = dict(solved=0, rhs=0, inst=0, steps_solved=[])
     evs = []
     with Clocks(local) as clk:
         barrier()
@@ -253,6 +264,7 @@ def run_ours(args):
             totals["solved"] += int((r["status"] == 0).sum())
             totals["rhs"] += int(r["rhs"].sum())
             totals["inst"] += len(set(pidx[r["status"] == 0]))
+            totals["steps_solved"] += list(r["steps"][r["status"] == 0])
         barrier()
     clocks = clk.summary()
     step_ms = [a.elapsed_time(c) for a, _, c in evs]
@@ -269,6 +281,8 @@ def run_ours(args):
         sums = ss.cpu().numpy()
     solved_all, rhs_all, inst_all = sums
 
+    rhs_line = rhs_kernel_bench(A, probs[0], ics_dev, nm, st) if not args.no_rhs_bench else None
+
     # end to end through the C ABI from pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -284,7 +298,8 @@ def run_ours(args):
             solver.Solve()
             r = solver.results()
             solver.GetSatStates(np.float32, out=host_out)
-            e_solved += int((r["status"] == 0).sum())
+            e_solved += (int((r["status"] == 0).sum()) if args.all_trajectories
+                         else len(set(pidx[r["status"] == 0])))
         barrier()
         t_e = time.perf_counter() - t0
         if dist is not None:
@@ -311,12 +326,14 @@ def run_ours(args):
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     kern_s = sum(kern_ms) / 1e3
     achieved = (totals["rhs"] * B_rhs) / kern_s / 1e9
+    headline = solved_all if args.all_trajectories else inst_all
     line = {
-        "metric": "solves/s", "value": solved_all / t_max, "unit": "solves/s",
+        "metric": "solves/s", "value": headline / t_max, "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": W["name"], "instances_per_gpu": args.instances,
+                   "stop_on_first": not args.all_trajectories,
                    "trajectories_per_instance": args.traj, "N": W["n"], "M": W["m"], "K": W["k"],
                    "eps": W["eps"], "batch": W["batch"], "max_steps": W["maxsteps"],
                    "state": "fp32, a in log space, fp64 error norm/time",
@@ -324,7 +341,12 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}"},
         "rhs_evals_per_s": rhs_all / t_max,
         "instances_solved_per_s": inst_all / t_max,
-        "solved_fraction": totals["solved"] / (len(pidx) * args.steps),
+        "trajectory_solves_per_s": solved_all / t_max,
+        "instances_solved_fraction": totals["inst"] / (args.instances * args.steps),
+        "median_steps_of_solved_trajectories": float(np.median(totals["steps_solved"]))
+        if totals["steps_solved"] else None,
+        "mode": "all trajectories to their own result" if args.all_trajectories
+        else "first solution per instance stops its other trajectories",
         "gpu_launches": args.steps * len(solver_groups(solver)),
         "roofline": {"bound": "hbm", "kernel": "solve_kernel", "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
@@ -336,6 +358,10 @@ def run_ours(args):
     }
     if e2e:
         line["e2e"] = e2e
+    if rhs_line:
+        rhs_line["peak"] = hbm_peak
+        rhs_line["frac"] = rhs_line["achieved"] / hbm_peak
+        line["rhs_roofline"] = rhs_line
     if world == 1 and not args.no_cpu_baseline:
         try:
             c = cpu_baseline(probs_raw, pidx, ics, args.cpu_sample_seconds)
@@ -351,6 +377,33 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def rhs_kernel_bench(A, problem, ics_dev, nm, st, reps=10):
+    """Standalone batched RHS (ISat::GetDerivatives) over every trajectory's state,
+    state in HBM (16,384 x 5,250 FP32 = 344 MB in, 344 MB out per launch)."""
+    import torch
+    x = ics_dev.view(-1, nm)
+    out = torch.empty_like(x)
+    B = x.shape[0]
+    W = WORKLOAD
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            A.get_derivatives(problem, x, out=out, logspace=False, stream=st.cuda_stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            A.get_derivatives(problem, x, out=out, logspace=False, stream=st.cuda_stream)
+        e1.record(st)
+    st.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    # algorithmic bytes: state in + derivative out, and the instance's literal stream once
+    # per launch (T_share = all B states of the launch)
+    bytes_per_launch = B * 8 * nm + 4 * W["k"] * W["m"]
+    return {"bound": "hbm", "kernel": "rhs_batch_kernel", "states_per_launch": B,
+            "ms_per_launch": ms, "achieved": bytes_per_launch / (ms / 1e3) / 1e9, "unit": "GB/s",
+            "bytes_per_launch": bytes_per_launch, "traffic": None}
 
 
 def solver_groups(solver):

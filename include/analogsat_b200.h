@@ -52,7 +52,7 @@ extern "C" {
 #define AS_ERR_IO (-5)
 
 /* numeric modes */
-#define AS_PREC_F32_LOGA 0 /* FP32 state, a_m held as ln a_m, FP64 error norm + time */
+#define AS_PREC_F32_LOGA 0 /* FP32 state, a_m held as log2 a_m, FP64 error norm + time */
 #define AS_PREC_F64 1      /* FP64 state, linear a_m: bit-for-bit the reference RHS */
 
 typedef struct as_problem as_problem;
@@ -92,7 +92,7 @@ void as_problem_free(as_problem* p);
 /* ISat::GetDerivatives over `num_states` states at once (CpuSat.cpp:65-94,
  * CudaSat1.cu:501-531).  x and dxdt are DEVICE pointers to num_states public-layout
  * vectors of N+M values each (FP32).  logspace = 1: the a-block of x holds
- * u = ln a and receives du/dt = K^2. */
+ * u = log2 a and receives du/dt = K^2 / ln 2 (the solver's internal form). */
 int32_t as_rhs_f32(as_problem* p, const float* x, float* dxdt, int32_t num_states,
                    int32_t logspace, void* stream);
 /* FP64 variant, linear a: bit-identical to CpuSat<double>::GetDerivatives. */

@@ -341,6 +341,27 @@ int orc_solve(const orc_problem* p, const double* ic, double eps, double tmax, i
     return result;
 }
 
+/* Dense-output reference: the same controller, but the last step is clamped so the
+ * integration ends at t_end (used to compare runs whose step sequences differ). */
+int orc_integrate_to(const orc_problem* p, const double* ic, double eps, double t_end,
+                     int logspace, int maxsteps, double* out_state, double* out_time) {
+    rk_t rk;
+    int s = 0;
+    double* x = (double*)malloc(sizeof(double) * (size_t)(p->n + p->m + 1));
+    rk_init(&rk, p, eps, logspace);
+    load_ic(p, ic, x, logspace);
+    while (rk.time < t_end && s < maxsteps) {
+        if (rk.time + rk.hnext > t_end) rk.hnext = t_end - rk.time;
+        if (!rk_step(&rk, x)) break;
+        s++;
+    }
+    store_pub(p, x, out_state, logspace);
+    *out_time = rk.time;
+    rk_free(&rk);
+    free(x);
+    return s;
+}
+
 double orc_potential(const orc_problem* p, const double* x, const double* w) {
     int j, q;
     double v = 0.0;

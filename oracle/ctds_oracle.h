@@ -44,6 +44,10 @@ int orc_solve(const orc_problem* p, const double* ic, double eps, double tmax, i
               int batch, int logspace, double* final_state, double* out_time, int* out_steps,
               int* out_rhs, int* out_attempts, int* out_viol);
 
+/* Same integrator, final step clamped to end exactly at t_end; returns steps taken. */
+int orc_integrate_to(const orc_problem* p, const double* ic, double eps, double t_end,
+                     int logspace, int maxsteps, double* out_state, double* out_time);
+
 /* Potential V = sum_m w_m a_m K_m^2 of a public state (a linear). */
 double orc_potential(const orc_problem* p, const double* x, const double* w);
 

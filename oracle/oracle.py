@@ -62,6 +62,9 @@ class Oracle:
         L.orc_solve.argtypes = [C.c_void_p, _f64p, C.c_double, C.c_double, C.c_int, C.c_int,
                                 C.c_int, _f64p, C.POINTER(C.c_double), C.POINTER(C.c_int),
                                 C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.orc_integrate_to.restype = C.c_int
+        L.orc_integrate_to.argtypes = [C.c_void_p, _f64p, C.c_double, C.c_double, C.c_int, C.c_int,
+                                       _f64p, C.POINTER(C.c_double)]
         L.orc_potential.restype = C.c_double
         L.orc_potential.argtypes = [C.c_void_p, _f64p, C.c_void_p]
         self.L = L
@@ -114,6 +117,13 @@ class Oracle:
                                C.byref(a), C.byref(v))
         return dict(result=res, state=fin, time=t.value, steps=st.value, rhs=r.value,
                     attempts=a.value, violations=v.value)
+
+    def integrate_to(self, p, ic, t_end, eps=1e-10, logspace=False, maxsteps=10_000_000):
+        out = np.zeros(p.n + p.m)
+        t = C.c_double()
+        steps = self.L.orc_integrate_to(p.h, np.ascontiguousarray(ic, np.float64), eps, t_end,
+                                        int(logspace), maxsteps, out, C.byref(t))
+        return dict(state=out, time=t.value, steps=steps)
 
     def potential(self, p, x, w=None):
         wp = None

@@ -59,11 +59,11 @@ def test_rhs_logspace(golden, tag):
     x[:, p.n:] = rng.uniform(0.5, 4.0, size=(x.shape[0], p.m))
     d_lin = get_derivatives(p, _cuda(x)).cpu().numpy()
     xl = x.copy()
-    xl[:, p.n:] = np.log(x[:, p.n:])
+    xl[:, p.n:] = np.log2(x[:, p.n:])
     d_log = get_derivatives(p, _cuda(xl, torch.float32), logspace=True).cpu().numpy()
     for a, b, xx in zip(d_log, d_lin, x):
         assert np.abs(a[: p.n] - b[: p.n]).max() <= 1e-5 * np.abs(b[: p.n]).max()
-        du_ref = b[p.n:] / xx[p.n:]
+        du_ref = b[p.n:] / xx[p.n:] / np.log(2.0)
         assert np.abs(a[p.n:] - du_ref).max() <= 1e-5 * np.abs(du_ref).max() + 1e-30
 
 
@@ -155,21 +155,24 @@ def test_solver_f64_reference_solves(golden, tag):
     assert same >= len(ics) // 2
 
 
-def test_solver_f32_short_horizon_error(oracle, golden):
-    """FP32 state + log-space a vs an FP64 run of the same integrator (oracle, log
-    space) over 30 accepted steps of the N=1000, M=4250 instance."""
+@pytest.mark.parametrize("tag,nsteps", [("p200", 40), ("p1000", 30)])
+def test_solver_f32_short_horizon_error(oracle, golden, tag, nsteps):
+    """FP32 state + log-space a against the FP64 solution of the same ODE at the same
+    analog time (oracle integrated to the GPU's end time with eps 1e-10).  FP32 noise
+    in the error estimate changes the step sequence, so states are compared at equal
+    time, not equal step count.  Bound: 1e-5 relative (floor 1e-2 for near-zero spins)."""
     from analogsat_b200 import AS_PREC_F32_LOGA
-    ic = golden["p1000/traj_ic"]
-    s = _solver(golden, "p1000", AS_PREC_F32_LOGA, 1e-6, 30, 30)
+    ic = golden[f"{tag}/traj_ic"]
+    s = _solver(golden, tag, AS_PREC_F32_LOGA, 1e-6, nsteps, nsteps)
     s.SetSatStates([0], ic[None, :])
     s.Solve()
     r = s.results()
-    op = oracle.problem(golden["p1000/literals"], golden["p1000/lengths"])
-    o = oracle.solve(op, ic, eps=1e-6, maxsteps=30, batch=30, logspace=True)
-    assert r["steps"][0] == o["steps"] == 30
-    assert abs(r["time"][0] - o["time"]) <= 1e-5 * o["time"]
+    assert r["steps"][0] == nsteps
+    op = oracle.problem(golden[f"{tag}/literals"], golden[f"{tag}/lengths"])
+    o = oracle.integrate_to(op, ic, r["time"][0], eps=1e-10)
+    assert abs(o["time"] - r["time"][0]) <= 1e-12 * r["time"][0]
     x = s.GetSatState(0)
-    err = np.abs(x - o["state"]) / np.maximum(np.abs(o["state"]), 1e-3)
+    err = np.abs(x - o["state"]) / np.maximum(np.abs(o["state"]), 1e-2)
     assert err.max() <= 1e-5, err.max()
 
 
