@@ -119,21 +119,20 @@ using SolveFn = void (*)(SolveParams);
 
 struct Variant {
     int precision;  // AS_PREC_*
-    int kmax, bt;
+    int kmax;
+    bool exact;     // clause slots == kmax (no runtime length tests)
     SolveFn fn;
     size_t bytes_per_value;
 };
 
-#define AS_VARIANT_F32(K, BT) Variant{AS_PREC_F32_LOGA, K, BT, &solve_kernel<float, true, K, BT>, 4}
-#define AS_VARIANT_F64(K, BT) Variant{AS_PREC_F64, K, BT, &solve_kernel<double, false, K, BT>, 8}
+#define AS_VARIANT_F32(K, EX) Variant{AS_PREC_F32_LOGA, K, EX, &solve_kernel<float, true, K, EX>, 4}
+#define AS_VARIANT_F64(K, EX) Variant{AS_PREC_F64, K, EX, &solve_kernel<double, false, K, EX>, 8}
 
 const std::vector<Variant>& variants() {
     static const std::vector<Variant> v = {
-        AS_VARIANT_F32(3, 128),  AS_VARIANT_F32(3, 256),  AS_VARIANT_F32(3, 512),
-        AS_VARIANT_F32(3, 1024), AS_VARIANT_F32(4, 128),  AS_VARIANT_F32(4, 256),
-        AS_VARIANT_F32(4, 512),  AS_VARIANT_F32(4, 1024), AS_VARIANT_F32(16, 256),
-        AS_VARIANT_F32(16, 1024), AS_VARIANT_F64(3, 128), AS_VARIANT_F64(3, 256),
-        AS_VARIANT_F64(3, 512),  AS_VARIANT_F64(16, 256),
+        AS_VARIANT_F32(3, true),  AS_VARIANT_F32(4, true),  AS_VARIANT_F32(2, true),
+        AS_VARIANT_F32(16, false), AS_VARIANT_F64(3, true), AS_VARIANT_F64(4, true),
+        AS_VARIANT_F64(16, false),
     };
     return v;
 }
@@ -143,14 +142,18 @@ size_t solver_smem(const Variant& v, const PackedProblem& q) {
 }
 
 bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_limit) {
-    return q.compact && v.precision == precision && q.k <= v.kmax && solver_smem(v, q) <= smem_limit;
+    const bool kok = v.exact ? q.k == v.kmax : q.k <= v.kmax;
+    return q.compact && v.precision == precision && kok && solver_smem(v, q) <= smem_limit;
 }
 
-// Default CTA size: about four clauses per thread, 128..1024 threads.
+// CTA size: the smallest clause count per thread (at least 4) that keeps the CTA at
+// <= 1024 threads, then the fewest threads for that count (multiple of 32), so the
+// last clause iteration is nearly full.
 int preferred_bt(const PackedProblem& q) {
-    int bt = 128;
-    while (bt < 1024 && bt * 4 < q.m) bt *= 2;
-    return bt;
+    int c = 4;
+    while ((q.m + c - 1) / c > 1024) c++;
+    const int bt = ((q.m + c - 1) / c + 31) / 32 * 32;
+    return std::max(64, std::min(1024, bt));
 }
 
 __global__ void stamp_deadline_kernel(unsigned long long* out, unsigned long long budget_ns) {
@@ -195,7 +198,7 @@ struct as_solver {
     std::vector<long long> traj_bits;  // word offset into best_bits
     long long total_values = 0;
     std::vector<int> order;            // launch order -> user trajectory
-    struct Group { int variant, u0, u1; };
+    struct Group { int variant, u0, u1, bt; };
     std::vector<Group> groups;
 
     DevBuf states, results, unit_inst, unit_state, unit_bits, queue, solved, deadline, best_bits;
@@ -307,12 +310,12 @@ int ensure_uploaded(as_problem* p) {
     return p->dev.upload(v, dev);
 }
 
-template <typename T, bool LOGA, int KMAX>
+template <typename T, bool LOGA, int KMAX, bool EXACT>
 int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
     constexpr int BT = 512;
     const auto& q = p->packed;
     const size_t smem = rhs_smem_values(q.n, q.nslots) * sizeof(T);
-    auto fn = &rhs_batch_kernel<T, LOGA, KMAX, BT>;
+    auto fn = &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT>;
     int dev = 0, sms = 0, optin = 0, occ = 0;
     AS_CUDA(cudaGetDevice(&dev));
     AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -335,18 +338,18 @@ int dispatch_rhs(as_problem* p, const T* x, T* d, int ns, void* stream) {
     if (r) return r;
     cudaStream_t st = (cudaStream_t)stream;
     const int k = p->packed.k;
-    if (k <= 3) return launch_rhs<T, LOGA, 3>(p, x, d, ns, st);
-    if (k <= 4) return launch_rhs<T, LOGA, 4>(p, x, d, ns, st);
-    if (k <= 16) return launch_rhs<T, LOGA, 16>(p, x, d, ns, st);
+    if (k == 3) return launch_rhs<T, LOGA, 3, true>(p, x, d, ns, st);
+    if (k == 4) return launch_rhs<T, LOGA, 4, true>(p, x, d, ns, st);
+    if (k <= 16) return launch_rhs<T, LOGA, 16, false>(p, x, d, ns, st);
     return fail(AS_ERR_UNSUPPORTED, "clause length > 16 is not supported");
 }
 
-template <typename T, int KMAX>
+template <typename T, int KMAX, bool EXACT>
 int launch_viol(as_problem* p, const T* x, int* c, int ns, cudaStream_t st) {
     constexpr int BT = 256;
     const auto& q = p->packed;
     const size_t smem = (size_t)((q.n + 1 + 3) & ~3) * sizeof(T);
-    auto fn = &viol_batch_kernel<T, KMAX, BT>;
+    auto fn = &viol_batch_kernel<T, KMAX, EXACT, BT>;
     int dev = 0, sms = 0, optin = 0, occ = 0;
     AS_CUDA(cudaGetDevice(&dev));
     AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -368,9 +371,9 @@ int dispatch_viol(as_problem* p, const T* x, int* c, int ns, void* stream) {
     if (r) return r;
     cudaStream_t st = (cudaStream_t)stream;
     const int k = p->packed.k;
-    if (k <= 3) return launch_viol<T, 3>(p, x, c, ns, st);
-    if (k <= 4) return launch_viol<T, 4>(p, x, c, ns, st);
-    if (k <= 16) return launch_viol<T, 16>(p, x, c, ns, st);
+    if (k == 3) return launch_viol<T, 3, true>(p, x, c, ns, st);
+    if (k == 4) return launch_viol<T, 4, true>(p, x, c, ns, st);
+    if (k <= 16) return launch_viol<T, 16, false>(p, x, c, ns, st);
     return fail(AS_ERR_UNSUPPORTED, "clause length > 16 is not supported");
 }
 
@@ -524,13 +527,10 @@ int build_groups(as_solver* s) {
     for (int p = 0; p < np; p++) {
         const auto& q = s->problems[p];
         long best = -1;
-        const int want = s->forced_bt ? s->forced_bt : preferred_bt(q);
         for (int i = 0; i < (int)vs.size(); i++) {
             const auto& v = vs[i];
             if (!fits(v, q, s->precision, s->smem_limit)) continue;
-            if (s->forced_bt && v.bt != s->forced_bt) continue;
-            // closest CTA size to the preferred one, then the smallest KMAX that holds k
-            const long score = (long)std::abs(v.bt - want) * 1024 + v.kmax;
+            const long score = (v.exact ? 0 : 1000) + v.kmax;  // exact first, then smallest KMAX
             if (best < 0 || score < best) { best = score; pv[p] = i; }
         }
         if (pv[p] < 0)
@@ -547,9 +547,12 @@ int build_groups(as_solver* s) {
     s->groups.clear();
     for (int u = 0; u < num_traj;) {
         const int v = pv[pi[s->order[u]]];
-        int e = u;
-        while (e < num_traj && pv[pi[s->order[e]]] == v) e++;
-        s->groups.push_back({v, u, e});
+        int e = u, bt = 64;
+        while (e < num_traj && pv[pi[s->order[e]]] == v) {
+            bt = std::max(bt, preferred_bt(s->problems[pi[s->order[e]]]));
+            e++;
+        }
+        s->groups.push_back({v, u, e, s->forced_bt ? s->forced_bt : bt});
         u = e;
     }
     std::vector<int> ui(num_traj);
@@ -616,7 +619,7 @@ int record_solve(as_solver* s, cudaStream_t st) {
         }
         AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int occ = 0;
-        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.fn, v.bt, smem));
+        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.fn, G.bt, smem));
         if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
         const int units = G.u1 - G.u0;
         const int ctas = std::min(units, s->sm_count * occ);
@@ -638,8 +641,8 @@ int record_solve(as_solver* s, cudaStream_t st) {
         P.tmax = s->max_time;
         P.deadline = have_deadline ? s->deadline.as<unsigned long long>() : nullptr;
         void* args[] = {&P};
-        AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(v.bt), args, smem, st));
-        s->last_bt = v.bt; s->last_ctas = ctas; s->last_smem = (int)smem; s->last_occ = occ;
+        AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(G.bt), args, smem, st));
+        s->last_bt = G.bt; s->last_ctas = ctas; s->last_smem = (int)smem; s->last_occ = occ;
     }
     return AS_OK;
 }
@@ -782,11 +785,8 @@ int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas
 
 int32_t as_solver_force_threads(as_solver* s, int32_t threads) {
     if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
-    if (threads != 0) {
-        bool any = false;
-        for (auto& v : variants()) any = any || (v.precision == s->precision && v.bt == threads);
-        if (!any) return fail(AS_ERR_UNSUPPORTED, "no compiled variant with that CTA size");
-    }
+    if (threads != 0 && (threads < 32 || threads > 1024 || threads % 32 != 0))
+        return fail(AS_ERR_BAD_INPUT, "CTA size must be a multiple of 32 in [32, 1024]");
     s->forced_bt = threads;
     s->groups_dirty = true;
     s->invalidate();

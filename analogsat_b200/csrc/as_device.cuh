@@ -71,21 +71,24 @@ __device__ __forceinline__ int32_t ld_ro(const int32_t* p) {
 }
 
 // Clause phase for one clause m: stores the per-literal spin contributions into cs
-// and returns da_m (du_m in log space).  `am` is a_m in linear space.  KMAX bounds
-// the runtime clause length k.  For k <= 10 the leave-one-out products follow
-// CpuProdWrapper (ascending, left-associated); for k > 10 the generic CalculateAll
-// form (CpuSat.cpp:291-349).
-template <typename T, bool LOGA, int KMAX>
+// and returns da_m (du_m in log space).  `am` is a_m in linear space.
+// EXACT: every clause has exactly KMAX slots (shorter clauses are padded with the
+// sentinel word, whose contribution goes to the trash slot), so no runtime length
+// tests are needed; otherwise the runtime length k <= KMAX is honoured.  For
+// k <= 10 the leave-one-out products follow CpuProdWrapper (ascending,
+// left-associated); for k > 10 the generic CalculateAll form (CpuSat.cpp:291-349).
+template <typename T, bool LOGA, int KMAX, bool EXACT>
 __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* __restrict__ sy,
                                           T* __restrict__ cs, T am, T knorm) {
     using A = Arith<T>;
     uint32_t w[KMAX];
     T f[KMAX];
     T km = knorm;
+    const uint32_t* lp = I.lit + m;
 #pragma unroll
     for (int q = 0; q < KMAX; q++) {
-        if (q < I.k) {
-            w[q] = ld_ro(I.lit + q * I.mp + m);
+        if (EXACT || q < I.k) {
+            w[q] = ld_ro(lp + q * I.mp);
             const T s = sy[lit_var(w[q])];
             f[q] = lit_neg(w[q]) ? A::add(T(1), s) : A::sub(T(1), s);
             km = A::mul(km, f[q]);
@@ -98,12 +101,12 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
         const T r = A::mul(A::mul(km, knorm), am);
 #pragma unroll
         for (int q = 0; q < KMAX; q++) {
-            if (q < I.k && lit_slot(w[q]) != 0xffffu) {
+            if (EXACT || q < I.k) {
                 T prod = T(1);
                 bool first = true;
 #pragma unroll
                 for (int l = 0; l < KMAX; l++) {
-                    if (l != q && l < I.k) {
+                    if (l != q && (EXACT || l < I.k)) {
                         prod = first ? f[l] : A::mul(prod, f[l]);
                         first = false;
                     }
@@ -116,11 +119,11 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
     } else {
 #pragma unroll
         for (int q = 0; q < KMAX; q++) {
-            if (q < I.k && lit_slot(w[q]) != 0xffffu) {
+            if (EXACT || q < I.k) {
                 T temp = km;
 #pragma unroll
                 for (int l = 0; l < KMAX; l++)
-                    if (l < I.k) temp = A::mul(temp, l == q ? T(1) : f[l]);
+                    if (EXACT || l < I.k) temp = A::mul(temp, l == q ? T(1) : f[l]);
                 const T rr = A::mul(A::mul(A::mul(T(2), temp), knorm), am);
                 cs[lit_slot(w[q])] = lit_neg(w[q]) ? -rr : rr;
             }
@@ -138,18 +141,19 @@ __device__ __forceinline__ T var_phase(const DevInstance& I, int v, const T* __r
     const int r0 = ld_ro(I.srow + g), r1 = ld_ro(I.srow + g + 1);
     const T* p = cs + r0 * 32 + (v & 31);
     T sum = T(0);
+#pragma unroll 4
     for (int r = r0; r < r1; r++, p += 32) sum = A::add(sum, *p);
     return sum;
 }
 
 // Clause check for clause m against the spins in sy (CpuSat.cpp:136-164): a
 // variable is TRUE when s > 0; the sentinel (s = -1, positive) is FALSE.
-template <int KMAX, typename T>
+template <int KMAX, bool EXACT, typename T>
 __device__ __forceinline__ int clause_violated(const DevInstance& I, int m, const T* sy) {
     bool sat = false;
 #pragma unroll
     for (int q = 0; q < KMAX; q++) {
-        if (q < I.k) {
+        if (EXACT || q < I.k) {
             const uint32_t w = ld_ro(I.lit + q * I.mp + m);
             const bool t = sy[lit_var(w)] > T(0);
             sat |= lit_neg(w) ? !t : t;
@@ -159,7 +163,7 @@ __device__ __forceinline__ int clause_violated(const DevInstance& I, int m, cons
 }
 
 // ---- block reductions (warp shuffles + one smem slot per warp) ----
-template <int BT>
+// red holds one slot per warp of the launch (blockDim.x / 32 <= 32).
 __device__ __forceinline__ int block_sum(int v, int* red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -168,14 +172,13 @@ __device__ __forceinline__ int block_sum(int v, int* red) {
     if (lane == 0) red[warp] = v;
     __syncthreads();
     int s = 0;
-#pragma unroll
-    for (int w = 0; w < BT / 32; w++) s += red[w];
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
     return s;
 }
 
 // Block max (FP64) whose result is post-processed by thread 0: fn(max) is broadcast
-// to every thread; fn may publish more values in red[BT/32 + 1 ...].
-template <int BT, typename F>
+// to every thread through red[32]; fn may publish more values in red[33...].
+template <typename F>
 __device__ __forceinline__ double block_max_then(double v, double* red, F&& fn) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -185,12 +188,11 @@ __device__ __forceinline__ double block_max_then(double v, double* red, F&& fn) 
     __syncthreads();
     if (threadIdx.x == 0) {
         double m = red[0];
-#pragma unroll
-        for (int w = 1; w < BT / 32; w++) m = fmax(m, red[w]);
-        red[BT / 32] = fn(m);
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmax(m, red[w]);
+        red[32] = fn(m);
     }
     __syncthreads();
-    return red[BT / 32];
+    return red[32];
 }
 
 }  // namespace asb

@@ -1,11 +1,10 @@
 // Kernels of the AnalogSAT B200 hot path.
 //
 //  solve_kernel    persistent RK45 (Cash-Karp) integrator: one CTA per trajectory,
-//                  work units popped from a global counter (dynamic refill), spins
-//                  and clause contributions staged in shared memory, all RK stage
-//                  vectors held in registers (thread c owns clauses c, c+BT, ... and
-//                  variables c, c+BT, ...), batched clause check and early exit on
-//                  device.  Replaces SatSolver::DoSolve + CpuRungeKutta::Step/rkqs/
+//                  work units popped from a global counter (dynamic refill); the
+//                  whole trajectory -- RK stage vectors, spins, clause contributions
+//                  -- lives in shared memory for its lifetime; batched clause check
+//                  and early exit on device.  Replaces SatSolver::DoSolve + CpuRungeKutta::Step/rkqs/
 //                  rkck + CpuSat::GetDerivatives/GetClauseViolationCount
 //                  (AnalogSAT/solver/SatSolver.h:273-355,
 //                  AnalogSAT/cpu_sat/CpuRungeKutta.cpp:66-100,181-267,
@@ -131,7 +130,6 @@ __device__ __forceinline__ float rk_err_ratio(float x, float k1, float k3, float
     return __fdividef(fabsf(e), sc);
 }
 
-template <int BT>
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -146,7 +144,7 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 //   X, K1..K5   the RK stage vectors (state, k1..k5), E values each;
 //   sy          the stage's spin vector plus the sentinel slot sy[n] = -1;
 //   cs          SELL-32 contribution slots (nslots values, padding kept at 0).
-// Element e is owned by thread e % BT in every stage loop, so stage vectors need no
+// Element e is owned by thread e % blockDim.x in every stage loop, so stage vectors need no
 // barriers; only sy and cs are exchanged between threads.
 template <typename T>
 struct Stages {
@@ -155,10 +153,10 @@ struct Stages {
 
 __host__ __device__ inline size_t solve_smem_values(int n, int m, int nslots) {
     const size_t E = (size_t)((n + m + 3) & ~3);
-    return 6 * E + (size_t)((n + 1 + 3) & ~3) + (size_t)nslots;
+    return 6 * E + (size_t)((n + 1 + 3) & ~3) + (size_t)nslots + 1;
 }
 
-template <typename T, bool LOGA, int KMAX, int BT>
+template <typename T, bool LOGA, int KMAX, bool EXACT>
 struct Solver {
     using A = Arith<T>;
     using ET = T;  // error-ratio type (see rk_err_ratio)
@@ -169,19 +167,19 @@ struct Solver {
     template <int S>
     static __device__ __forceinline__ void eval(const DevInstance& I, T* sy, T* cs, T knorm,
                                                 const Stages<T>& st, T hT, T h0T, ET& errmax) {
-        const int tid = threadIdx.x;
+        const int tid = threadIdx.x, nt = blockDim.x;
         const int n = I.n;
-        for (int v = tid; v < n; v += BT)
+        for (int v = tid; v < n; v += nt)
             sy[v] = stage_in<S>(st.X[v], st.K1[v], st.K2[v], st.K3[v], st.K4[v], st.K5[v], hT);
         __syncthreads();
-        for (int m = tid; m < I.m; m += BT) {
+        for (int m = tid; m < I.m; m += nt) {
             const int e = n + m;
             const T x = st.X[e];
             const T y = stage_in<S>(x, st.K1[e], st.K2[e], st.K3[e], st.K4[e], st.K5[e], hT);
             T am;
             if constexpr (LOGA) am = exp2_fast(y);
             else am = y;
-            const T d = clause_phase<T, LOGA, KMAX>(I, m, sy, cs, am, knorm);
+            const T d = clause_phase<T, LOGA, KMAX, EXACT>(I, m, sy, cs, am, knorm);
             if constexpr (S == 1) st.K1[e] = d;
             if constexpr (S == 2) st.K2[e] = d;
             if constexpr (S == 3) st.K3[e] = d;
@@ -194,7 +192,7 @@ struct Solver {
             }
         }
         __syncthreads();
-        for (int v = tid; v < n; v += BT) {
+        for (int v = tid; v < n; v += nt) {
             const T d = var_phase<T>(I, v, cs);
             if constexpr (S == 1) st.K1[v] = d;
             if constexpr (S == 2) st.K2[v] = d;
@@ -210,15 +208,17 @@ struct Solver {
     }
 };
 
-template <typename T, bool LOGA, int KMAX, int BT>
-__global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel(SolveParams P) {
+// Any block size that is a multiple of 32 and at most 1024 works; the host picks it
+// so that every thread handles about the same number of clauses.
+template <typename T, bool LOGA, int KMAX, bool EXACT>
+__global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
     using A = Arith<T>;
-    using S = Solver<T, LOGA, KMAX, BT>;
+    using S = Solver<T, LOGA, KMAX, EXACT>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[BT / 32 + 2];
-    __shared__ int red_i[BT / 32];
+    __shared__ double red_d[34];
+    __shared__ int red_i[32];
     __shared__ int s_unit, s_flag;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, nt = blockDim.x;
 
     while (true) {
         if (tid == 0) s_unit = atomicAdd(P.queue_head, 1);
@@ -237,13 +237,13 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
         const T knorm = (T)ldexp(1.0, -I.k);
 
         // initial state: public spins scattered to internal order; a -> log2 a
-        for (int i = tid; i < n; i += BT) st.X[__ldg(I.iperm + i)] = G[i];
-        for (int e = n + tid; e < E; e += BT) {
+        for (int i = tid; i < n; i += nt) st.X[__ldg(I.iperm + i)] = G[i];
+        for (int e = n + tid; e < E; e += nt) {
             const T a = G[e];
             if constexpr (LOGA) st.X[e] = log2f(a);
             else st.X[e] = a;
         }
-        for (int j = tid; j < I.nslots; j += BT) cs[j] = T(0);
+        for (int j = tid; j <= I.nslots; j += nt) cs[j] = T(0);
         if (tid == 0) sy[n] = T(-1);  // sentinel spin: padding literals are always FALSE
 
         double t = 0.0, hnext = 1e-9, hdid = 0.0;
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
                     attempts++;
                     // step-size control (CpuRungeKutta.cpp:229-259): one thread evaluates
                     // pow() and broadcasts the new step size with the error norm
-                    ermax = block_max_then<BT>((double)em, red_d, [&](double emax) {
+                    ermax = block_max_then((double)em, red_d, [&](double emax) {
                         const double e = __ddiv_rn(emax, P.eps);
                         double hn;
                         if (e <= 1.0)
@@ -287,10 +287,10 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
                         else
                             hn = fmax(__dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PSHRNK)),
                                       __dmul_rn(ck::HFACTOR, h));
-                        red_d[BT / 32 + 1] = hn;
+                        red_d[33] = hn;
                         return e;
                     });
-                    const double hn = red_d[BT / 32 + 1];
+                    const double hn = red_d[33];
                     if (ermax <= 1.0) { hnext = hn; break; }
                     h = hn;
                     if (__dadd_rn(t, h) == t) { underflow = true; break; }
@@ -306,16 +306,16 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
             steps += taken;
 
             // ---- CpuSat::GetClauseViolationCount on the accepted state ----
-            for (int v = tid; v < n; v += BT) sy[v] = st.X[v];
+            for (int v = tid; v < n; v += nt) sy[v] = st.X[v];
             __syncthreads();
             int cnt = 0;
-            for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX>(I, m, sy);
-            viol = block_sum<BT>(cnt, red_i);
+            for (int m = tid; m < I.m; m += nt) cnt += clause_violated<KMAX, EXACT>(I, m, sy);
+            viol = block_sum(cnt, red_i);
             if (viol < minviol) {
                 minviol = viol;
                 if (P.best_bits) {
                     uint32_t* bits = P.best_bits + P.unit_bits[u];
-                    for (int i0 = tid & ~31; i0 < n; i0 += BT) {
+                    for (int i0 = tid & ~31; i0 < n; i0 += nt) {
                         const int i = i0 + (tid & 31);
                         const bool b = i < n && sy[__ldg(I.iperm + (i < n ? i : 0))] > T(0);
                         const unsigned bal = __ballot_sync(0xffffffffu, b);
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
             }
             if (tid == 0) {
                 int f = 0;
-                if (P.deadline && globaltimer_ns<BT>() >= *P.deadline) f = 1;
+                if (P.deadline && globaltimer_ns() >= *P.deadline) f = 1;
                 if (P.stop_on_first && atomicAdd(P.inst_solved + pidx, 0) != 0) f = 1;
                 s_flag = f;
             }
@@ -344,8 +344,8 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
 
         // write back the final state in the public layout
         __syncthreads();
-        for (int i = tid; i < n; i += BT) G[i] = st.X[__ldg(I.iperm + i)];
-        for (int e = n + tid; e < E; e += BT) {
+        for (int i = tid; i < n; i += nt) G[i] = st.X[__ldg(I.iperm + i)];
+        for (int e = n + tid; e < E; e += nt) {
             const T v = st.X[e];
             if constexpr (LOGA) G[e] = exp2f(v);
             else G[e] = v;
@@ -367,10 +367,10 @@ __global__ void __launch_bounds__(BT, (BT >= 1024 ? 1 : 1024 / BT)) solve_kernel
 // internal variable order happens in shared memory.
 // ---------------------------------------------------------------------------
 __host__ __device__ inline size_t rhs_smem_values(int n, int nslots) {
-    return (size_t)((n + 1 + 3) & ~3) + (size_t)nslots;
+    return (size_t)((n + 1 + 3) & ~3) + (size_t)nslots + 1;
 }
 
-template <typename T, bool LOGA, int KMAX, int BT>
+template <typename T, bool LOGA, int KMAX, bool EXACT, int BT>
 __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* __restrict__ x,
                                                         T* __restrict__ dxdt, int ntraj,
                                                         long long stride) {
@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
     const int tid = threadIdx.x;
     const int n = I.n;
     const T knorm = (T)ldexp(1.0, -I.k);
-    for (int j = tid; j < I.nslots; j += BT) cs[j] = T(0);
+    for (int j = tid; j <= I.nslots; j += BT) cs[j] = T(0);
     for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
         const T* X = x + (long long)tr * stride;
         T* D = dxdt + (long long)tr * stride;
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
             T am;
             if constexpr (LOGA) am = exp2_fast(a);
             else am = a;
-            D[n + m] = clause_phase<T, LOGA, KMAX>(I, m, sy, cs, am, knorm);
+            D[n + m] = clause_phase<T, LOGA, KMAX, EXACT>(I, m, sy, cs, am, knorm);
         }
         __syncthreads();
         // ds in internal order -> sy (no longer read) -> public order, coalesced
@@ -404,12 +404,12 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
 }
 
 // Exact unsat counts of many states: one CTA per state.
-template <typename T, int KMAX, int BT>
+template <typename T, int KMAX, bool EXACT, int BT>
 __global__ void __launch_bounds__(BT) viol_batch_kernel(DevInstance I, const T* __restrict__ x,
                                                          int* __restrict__ counts, int ntraj,
                                                          long long stride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int red_i[BT / 32];
+    __shared__ int red_i[32];
     T* sy = reinterpret_cast<T*>(smem_raw);
     const int tid = threadIdx.x;
     for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
@@ -418,8 +418,8 @@ __global__ void __launch_bounds__(BT) viol_batch_kernel(DevInstance I, const T* 
         if (tid == 0) sy[I.n] = T(-1);
         __syncthreads();
         int cnt = 0;
-        for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX>(I, m, sy);
-        cnt = block_sum<BT>(cnt, red_i);
+        for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX, EXACT>(I, m, sy);
+        cnt = block_sum(cnt, red_i);
         if (tid == 0) counts[tr] = cnt;
         __syncthreads();
     }

@@ -120,9 +120,9 @@ PackedProblem pack(const HostProblem& p) {
         q.srow[g + 1] = q.srow[g] + w;
     }
     q.nslots = q.srow[q.nslices] * 32;
-    q.compact = p.n < 32768 && q.nslots < (int)kPadSlot;
+    q.compact = p.n < 32768 && q.nslots <= 65535;
 
-    const uint32_t pad = ((uint32_t)std::min(p.n, 32767) << 16) | kPadSlot;
+    const uint32_t pad = ((uint32_t)std::min(p.n, 32767) << 16) | (uint32_t)std::min(q.nslots, 65535);
     q.lit.assign((size_t)q.k * q.mp, pad);
     std::vector<int32_t> rank(p.n, 0);  // next row of each internal variable
     for (int j = 0; j < p.m; j++) {

@@ -20,11 +20,12 @@
 //        bit 31     negated literal
 //        bits 16-30 internal variable index
 //        bits 0-15  contribution slot of this literal
-//    Slots past a clause's length hold the sentinel word (var = N, slot 0xffff):
+//    Slots past a clause's length hold the sentinel word (var = N, slot = nslots):
 //    the sentinel spin is held at -1, so each contributes the factor 2 exactly like
 //    the reference's zero padding against its constant FALSE slot
-//    (CpuSat.cpp:214-215), and its contribution is dropped.
-//    This "compact" encoding needs N < 32768 and fewer than 65535 slots; larger
+//    (CpuSat.cpp:214-215), and its contribution lands in the never-read trash slot
+//    nslots, so the kernels store unconditionally.
+//    This "compact" encoding needs N < 32768 and at most 65535 slots; larger
 //    instances are rejected by the shared-memory kernels.
 #pragma once
 
@@ -49,13 +50,11 @@ bool read_cnf(const char* path, HostProblem& p, std::string& msg);
 // CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74).
 bool write_cnf(const char* path, const HostProblem& p);
 
-constexpr uint32_t kPadSlot = 0xffffu;
-
 struct PackedProblem {
     int n = 0, m = 0, k = 0;
     int mp = 0;          // clause stride: m rounded up to a multiple of 32
     int nslices = 0;     // ceil(n / 32)
-    int nslots = 0;      // srow[nslices] * 32
+    int nslots = 0;      // srow[nslices] * 32 (slot nslots is the trash slot)
     bool compact = false;
     std::vector<uint32_t> lit;     // [k][mp] literal words
     std::vector<int32_t> srow;     // [nslices + 1]

@@ -178,9 +178,9 @@ int32_t as_solver_get_best_assignment(as_solver* s, int32_t traj, uint32_t* bits
  * launched, dynamic shared memory per CTA and resident CTAs per SM. */
 int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas, int32_t* smem_bytes,
                                    int32_t* ctas_per_sm);
-/* Force the CTA size (128, 256, 512 or 1024 threads) of the next solves; 0 restores
- * the automatic choice (about four clauses per thread).  Used by the autotuner.
- * Fails with AS_ERR_UNSUPPORTED when no compiled variant has that size. */
+/* Force the CTA size (a multiple of 32 in [32, 1024]) of the next solves; 0 restores
+ * the automatic choice (the fewest threads that give every thread about the same
+ * clause count, at least four).  Used by the autotuner. */
 int32_t as_solver_force_threads(as_solver* s, int32_t threads);
 
 #ifdef __cplusplus
