@@ -126,6 +126,14 @@ class SatProblem:
         check(self._lib.as_problem_get_clauses(self._h, _ptr(lits), _ptr(lens)))
         return lits[:nl], lens[: self.m]
 
+    def layout_stats(self, precision: int = AS_PREC_F32_LOGA) -> dict:
+        a, b, d = C.c_int32(), C.c_int32(), C.c_int32()
+        c = C.c_int64()
+        check(self._lib.as_problem_layout_stats(self._h, precision, C.byref(a), C.byref(b),
+                                                C.byref(c), C.byref(d)))
+        return dict(nslots=a.value, max_degree=b.value, bank_wavefronts=c.value,
+                    compact=bool(d.value))
+
     def __del__(self):
         try:
             if self._h:

@@ -37,6 +37,7 @@ SIGNATURES = [
     ("as_problem_get_nmk", _i32, [_vp, _pi32, _pi32, _pi32]),
     ("as_problem_num_literals", _i32, [_vp]),
     ("as_problem_get_clauses", _i32, [_vp, _pi32, _pi32]),
+    ("as_problem_layout_stats", _i32, [_vp, _i32, _pi32, _pi32, C.POINTER(C.c_int64), _pi32]),
     ("as_problem_free", None, [_vp]),
     ("as_rhs_f32", _i32, [_vp, _vp, _vp, _i32, _i32, _vp]),
     ("as_rhs_f64", _i32, [_vp, _vp, _vp, _i32, _vp]),

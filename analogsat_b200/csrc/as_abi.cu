@@ -53,7 +53,7 @@ struct DevBuf {
 // Device copy of one or more packed instances in a single pool.
 struct DevicePool {
     int device = -1;
-    DevBuf lit, srow, perm, iperm, inst;
+    DevBuf lit, srow, perm, iperm, icperm, inst;
     std::vector<DevInstance> host_inst;
 
     template <typename V>
@@ -65,19 +65,21 @@ struct DevicePool {
     }
 
     int upload(const std::vector<const PackedProblem*>& pk, int dev) {
-        size_t nl = 0, nr = 0, np = 0;
+        size_t nl = 0, nr = 0, np = 0, nc = 0;
         for (auto* q : pk) {
             nl += q->lit.size();
             nr += q->srow.size();
             np += q->perm.size();
+            nc += q->icperm.size();
         }
         AS_CUDA(lit.alloc(std::max<size_t>(nl, 1) * 4));
         AS_CUDA(srow.alloc(std::max<size_t>(nr, 1) * 4));
         AS_CUDA(perm.alloc(std::max<size_t>(np, 1) * 4));
         AS_CUDA(iperm.alloc(std::max<size_t>(np, 1) * 4));
+        AS_CUDA(icperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
         host_inst.clear();
-        size_t ol = 0, orr = 0, op = 0;
+        size_t ol = 0, orr = 0, op = 0, oc = 0;
         for (auto* q : pk) {
             DevInstance d;
             d.n = q->n; d.m = q->m; d.k = q->k; d.mp = q->mp; d.nslices = q->nslices;
@@ -86,13 +88,15 @@ struct DevicePool {
             d.srow = srow.as<int32_t>() + orr;
             d.perm = perm.as<int32_t>() + op;
             d.iperm = iperm.as<int32_t>() + op;
+            d.icperm = icperm.as<int32_t>() + oc;
             int r;
             if ((r = put(lit, ol, q->lit)) || (r = put(srow, orr, q->srow)) || (r = put(perm, op, q->perm)) ||
-                (r = put(iperm, op, q->iperm)))
+                (r = put(iperm, op, q->iperm)) || (r = put(icperm, oc, q->icperm)))
                 return r;
             ol += q->lit.size();
             orr += q->srow.size();
             op += q->perm.size();
+            oc += q->icperm.size();
             host_inst.push_back(d);
         }
         AS_CUDA(cudaMemcpy(inst.p, host_inst.data(), sizeof(DevInstance) * host_inst.size(),
@@ -169,8 +173,13 @@ __global__ void stamp_deadline_kernel(unsigned long long* out, unsigned long lon
 // ---------------------------------------------------------------------------
 struct as_problem {
     HostProblem host;
-    PackedProblem packed;
-    DevicePool dev;  // lazily uploaded for the device primitives
+    PackedProblem packed[2];  // [AS_PREC_F32_LOGA]: literals may be reordered; [AS_PREC_F64]: not
+    DevicePool dev[2];        // lazily uploaded for the device primitives
+
+    void pack_all() {
+        packed[AS_PREC_F32_LOGA] = pack(host, true);
+        packed[AS_PREC_F64] = pack(host, false);
+    }
 };
 
 struct as_solver {
@@ -242,7 +251,7 @@ int32_t as_problem_create(const int32_t* literals, const int32_t* lengths, int32
         if (lengths[j] < 0) return fail(AS_ERR_BAD_INPUT, "as_problem_create: negative clause length");
     auto* p = new as_problem();
     p->host.add_clauses(literals, lengths, num_clauses);
-    p->packed = pack(p->host);
+    p->pack_all();
     *out = p;
     return AS_OK;
 }
@@ -260,7 +269,7 @@ int32_t as_problem_read_cnf(const char* path, as_problem** out, char* msg, int32
         delete p;
         return fail(AS_ERR_IO, "as_problem_read_cnf: " + m);
     }
-    p->packed = pack(p->host);
+    p->pack_all();
     *out = p;
     return AS_OK;
 }
@@ -293,28 +302,41 @@ int32_t as_problem_get_clauses(const as_problem* p, int32_t* literals, int32_t* 
     return AS_OK;
 }
 
+int32_t as_problem_layout_stats(const as_problem* p, int32_t precision, int32_t* nslots,
+                                int32_t* max_degree, int64_t* bank_wavefronts, int32_t* compact) {
+    if (!p || (precision != AS_PREC_F32_LOGA && precision != AS_PREC_F64))
+        return fail(AS_ERR_BAD_INPUT, "as_problem_layout_stats: bad argument");
+    const auto& q = p->packed[precision];
+    if (nslots) *nslots = q.nslots;
+    if (max_degree) *max_degree = q.max_degree;
+    if (bank_wavefronts) *bank_wavefronts = q.bank_wavefronts;
+    if (compact) *compact = q.compact ? 1 : 0;
+    return AS_OK;
+}
+
 void as_problem_free(as_problem* p) { delete p; }
 
 // ---- device primitives ----
 namespace {
 
-int ensure_uploaded(as_problem* p) {
+int ensure_uploaded(as_problem* p, int prec) {
     if (p->host.m == 0 || p->host.k == 0) return fail(AS_ERR_NO_PROBLEM, "SAT problem has not been set");
-    if (!p->packed.compact)
+    if (!p->packed[prec].compact)
         return fail(AS_ERR_UNSUPPORTED, "instance too large for the shared-memory kernels "
                                         "(needs N < 32768 and < 65535 contribution slots)");
     int dev = 0;
     AS_CUDA(cudaGetDevice(&dev));
-    if (p->dev.device == dev) return AS_OK;
-    std::vector<const PackedProblem*> v{&p->packed};
-    return p->dev.upload(v, dev);
+    if (p->dev[prec].device == dev) return AS_OK;
+    std::vector<const PackedProblem*> v{&p->packed[prec]};
+    return p->dev[prec].upload(v, dev);
 }
 
 template <typename T, bool LOGA, int KMAX, bool EXACT>
 int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
     constexpr int BT = 512;
-    const auto& q = p->packed;
-    const size_t smem = rhs_smem_values(q.n, q.nslots) * sizeof(T);
+    constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
+    const auto& q = p->packed[prec];
+    const size_t smem = rhs_smem_values(q.n, q.m, q.nslots) * sizeof(T);
     auto fn = &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT>;
     int dev = 0, sms = 0, optin = 0, occ = 0;
     AS_CUDA(cudaGetDevice(&dev));
@@ -325,7 +347,7 @@ int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
     AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
     const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
-    fn<<<grid, BT, smem, st>>>(p->dev.host_inst[0], x, d, ns, (long long)(q.n + q.m));
+    fn<<<grid, BT, smem, st>>>(p->dev[prec].host_inst[0], x, d, ns, (long long)(q.n + q.m));
     AS_CUDA(cudaGetLastError());
     return AS_OK;
 }
@@ -334,10 +356,11 @@ template <typename T, bool LOGA>
 int dispatch_rhs(as_problem* p, const T* x, T* d, int ns, void* stream) {
     if (!p || !x || !d || ns < 0) return fail(AS_ERR_BAD_INPUT, "as_rhs: null argument");
     if (ns == 0) return AS_OK;
-    int r = ensure_uploaded(p);
+    constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
+    int r = ensure_uploaded(p, prec);
     if (r) return r;
     cudaStream_t st = (cudaStream_t)stream;
-    const int k = p->packed.k;
+    const int k = p->packed[prec].k;
     if (k == 3) return launch_rhs<T, LOGA, 3, true>(p, x, d, ns, st);
     if (k == 4) return launch_rhs<T, LOGA, 4, true>(p, x, d, ns, st);
     if (k <= 16) return launch_rhs<T, LOGA, 16, false>(p, x, d, ns, st);
@@ -347,7 +370,8 @@ int dispatch_rhs(as_problem* p, const T* x, T* d, int ns, void* stream) {
 template <typename T, int KMAX, bool EXACT>
 int launch_viol(as_problem* p, const T* x, int* c, int ns, cudaStream_t st) {
     constexpr int BT = 256;
-    const auto& q = p->packed;
+    constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
+    const auto& q = p->packed[prec];
     const size_t smem = (size_t)((q.n + 1 + 3) & ~3) * sizeof(T);
     auto fn = &viol_batch_kernel<T, KMAX, EXACT, BT>;
     int dev = 0, sms = 0, optin = 0, occ = 0;
@@ -358,7 +382,7 @@ int launch_viol(as_problem* p, const T* x, int* c, int ns, cudaStream_t st) {
     AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
     const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
-    fn<<<grid, BT, smem, st>>>(p->dev.host_inst[0], x, c, ns, (long long)(q.n + q.m));
+    fn<<<grid, BT, smem, st>>>(p->dev[prec].host_inst[0], x, c, ns, (long long)(q.n + q.m));
     AS_CUDA(cudaGetLastError());
     return AS_OK;
 }
@@ -367,10 +391,11 @@ template <typename T>
 int dispatch_viol(as_problem* p, const T* x, int* c, int ns, void* stream) {
     if (!p || !x || !c || ns < 0) return fail(AS_ERR_BAD_INPUT, "as_violations: null argument");
     if (ns == 0) return AS_OK;
-    int r = ensure_uploaded(p);
+    constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
+    int r = ensure_uploaded(p, prec);
     if (r) return r;
     cudaStream_t st = (cudaStream_t)stream;
-    const int k = p->packed.k;
+    const int k = p->packed[prec].k;
     if (k == 3) return launch_viol<T, 3, true>(p, x, c, ns, st);
     if (k == 4) return launch_viol<T, 4, true>(p, x, c, ns, st);
     if (k <= 16) return launch_viol<T, 16, false>(p, x, c, ns, st);
@@ -414,7 +439,7 @@ int32_t as_solver_create(const as_problem* const* problems, int32_t num_problems
     int r = current_device(device, &s->device);
     if (r) return r;
     s->precision = precision;
-    for (int i = 0; i < num_problems; i++) s->problems.push_back(problems[i]->packed);
+    for (int i = 0; i < num_problems; i++) s->problems.push_back(problems[i]->packed[precision]);
     std::vector<const PackedProblem*> pk;
     for (auto& q : s->problems) pk.push_back(&q);
     r = s->pool.upload(pk, s->device);

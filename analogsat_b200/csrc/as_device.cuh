@@ -27,8 +27,9 @@ struct DevInstance {
     int n, m, k, mp, nslices, nslots;
     const uint32_t* lit;   // [k][mp] literal words (var | sign | slot)
     const int32_t* srow;   // [nslices + 1] SELL row offsets
-    const int32_t* perm;   // internal -> public variable
-    const int32_t* iperm;  // public -> internal variable
+    const int32_t* perm;    // internal -> public variable
+    const int32_t* iperm;   // public -> internal variable
+    const int32_t* icperm;  // public -> internal clause
 };
 
 constexpr float kInvLn2 = 1.4426950408889634f;  // d(log2 a)/dt = (da/dt) / (a ln 2)

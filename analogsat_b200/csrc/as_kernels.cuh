@@ -238,8 +238,9 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
 
         // initial state: public spins scattered to internal order; a -> log2 a
         for (int i = tid; i < n; i += nt) st.X[__ldg(I.iperm + i)] = G[i];
-        for (int e = n + tid; e < E; e += nt) {
-            const T a = G[e];
+        for (int j = tid; j < I.m; j += nt) {
+            const T a = G[n + j];
+            const int e = n + __ldg(I.icperm + j);
             if constexpr (LOGA) st.X[e] = log2f(a);
             else st.X[e] = a;
         }
@@ -345,10 +346,10 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         // write back the final state in the public layout
         __syncthreads();
         for (int i = tid; i < n; i += nt) G[i] = st.X[__ldg(I.iperm + i)];
-        for (int e = n + tid; e < E; e += nt) {
-            const T v = st.X[e];
-            if constexpr (LOGA) G[e] = exp2f(v);
-            else G[e] = v;
+        for (int j = tid; j < I.m; j += nt) {
+            const T v = st.X[n + __ldg(I.icperm + j)];
+            if constexpr (LOGA) G[n + j] = exp2f(v);
+            else G[n + j] = v;
         }
         if (tid == 0) {
             UnitResult r;
@@ -366,8 +367,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
 // layout).  Reads of x and writes of dxdt are coalesced; the permutation to the
 // internal variable order happens in shared memory.
 // ---------------------------------------------------------------------------
-__host__ __device__ inline size_t rhs_smem_values(int n, int nslots) {
-    return (size_t)((n + 1 + 3) & ~3) + (size_t)nslots + 1;
+__host__ __device__ inline size_t rhs_smem_values(int n, int m, int nslots) {
+    return (size_t)((n + 1 + 3) & ~3) + (size_t)((m + 3) & ~3) + (size_t)nslots + 1;
 }
 
 template <typename T, bool LOGA, int KMAX, bool EXACT, int BT>
@@ -376,7 +377,8 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
                                                         long long stride) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* sy = reinterpret_cast<T*>(smem_raw);
-    T* cs = sy + ((I.n + 1 + 3) & ~3);
+    T* ab = sy + ((I.n + 1 + 3) & ~3);  // clause weights in internal clause order
+    T* cs = ab + ((I.m + 3) & ~3);
     const int tid = threadIdx.x;
     const int n = I.n;
     const T knorm = (T)ldexp(1.0, -I.k);
@@ -384,21 +386,24 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
     for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
         const T* X = x + (long long)tr * stride;
         T* D = dxdt + (long long)tr * stride;
+        // coalesced reads, permuted into the internal orders in shared memory
         for (int i = tid; i < n; i += BT) sy[__ldg(I.iperm + i)] = X[i];
+        for (int j = tid; j < I.m; j += BT) ab[__ldg(I.icperm + j)] = X[n + j];
         if (tid == 0) sy[n] = T(-1);
         __syncthreads();
         for (int m = tid; m < I.m; m += BT) {
-            const T a = X[n + m];
+            const T a = ab[m];
             T am;
             if constexpr (LOGA) am = exp2_fast(a);
             else am = a;
-            D[n + m] = clause_phase<T, LOGA, KMAX, EXACT>(I, m, sy, cs, am, knorm);
+            ab[m] = clause_phase<T, LOGA, KMAX, EXACT>(I, m, sy, cs, am, knorm);
         }
         __syncthreads();
         // ds in internal order -> sy (no longer read) -> public order, coalesced
         for (int v = tid; v < n; v += BT) sy[v] = var_phase<T>(I, v, cs);
         __syncthreads();
         for (int i = tid; i < n; i += BT) D[i] = sy[__ldg(I.iperm + i)];
+        for (int j = tid; j < I.m; j += BT) D[n + j] = ab[__ldg(I.icperm + j)];
         __syncthreads();
     }
 }

@@ -89,7 +89,113 @@ bool write_cnf(const char* path, const HostProblem& p) {
     return true;
 }
 
-PackedProblem pack(const HostProblem& p) {
+namespace {
+
+// Greedy bank-aware grouping of clauses into warps of 32 (see as_problem.h): take
+// clauses in a shuffled order, put a clause into the open group when its literal
+// banks (optionally after reordering its literals) are all still free in their
+// slots; when no candidate within a search window fits, complete the group with the
+// least-conflicting candidates.  Deterministic (fixed seed).
+void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
+                      std::vector<std::vector<int8_t>>& order) {
+    const int m = p.m, k = p.k;
+    order.assign(m, {});
+    q.cperm.resize(m);
+    q.icperm.resize(m);
+    std::vector<int32_t> bank(p.storage.size());
+    for (size_t i = 0; i < p.storage.size(); i++) bank[i] = q.iperm[std::abs(p.storage[i]) - 1] & 31;
+    // candidate literal orders per clause length (all permutations for k <= 4)
+    auto perms_for = [&](int len) {
+        std::vector<std::vector<int8_t>> ps;
+        std::vector<int8_t> id(len);
+        for (int i = 0; i < len; i++) id[i] = (int8_t)i;
+        if (!permute || len > 4) { ps.push_back(id); return ps; }
+        do ps.push_back(id); while (std::next_permutation(id.begin(), id.end()));
+        return ps;
+    };
+    std::vector<std::vector<std::vector<int8_t>>> perms(k + 1);
+    for (int len = 1; len <= k; len++) perms[len] = perms_for(len);
+
+    std::vector<int32_t> rem(m);
+    for (int j = 0; j < m; j++) rem[j] = j;
+    uint64_t rng = 0x9E3779B97F4A7C15ull;
+    for (int j = m - 1; j > 0; j--) {  // Fisher-Yates with an xorshift generator
+        rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
+        std::swap(rem[j], rem[rng % (uint64_t)(j + 1)]);
+    }
+    const int kw = std::min(k, 16);
+    int out = 0;
+    long waves = 0;
+    std::vector<uint32_t> used(kw);
+    std::vector<int32_t> keep;
+    keep.reserve(m);
+    while (!rem.empty()) {
+        std::fill(used.begin(), used.end(), 0u);
+        int filled = 0;
+        keep.clear();
+        size_t scanned = 0;
+        auto cost = [&](int j, const std::vector<int8_t>& ord) {
+            int c = 0;
+            for (int qq = 0; qq < (int)ord.size() && qq < kw; qq++)
+                c += (used[qq] >> bank[p.start[j] + ord[qq]]) & 1u;
+            return c;
+        };
+        auto take = [&](int j, const std::vector<int8_t>& ord) {
+            for (int qq = 0; qq < (int)ord.size() && qq < kw; qq++)
+                used[qq] |= 1u << bank[p.start[j] + ord[qq]];
+            order[out] = ord;
+            q.cperm[out] = j;
+            out++;
+            filled++;
+        };
+        size_t i = 0;
+        for (; i < rem.size() && filled < 32; i++) {
+            const int j = rem[i];
+            bool placed = false;
+            if (scanned < 4096) {
+                scanned++;
+                for (const auto& ord : perms[p.length[j]])
+                    if (cost(j, ord) == 0) { take(j, ord); placed = true; break; }
+            }
+            if (!placed) keep.push_back(j);
+        }
+        for (; i < rem.size(); i++) keep.push_back(rem[i]);
+        while (filled < 32 && !keep.empty()) {
+            int best = 0, bc = 1 << 30;
+            const std::vector<int8_t>* bo = nullptr;
+            for (int c = 0; c < (int)keep.size() && c < 256; c++) {
+                for (const auto& ord : perms[p.length[keep[c]]]) {
+                    const int cc = cost(keep[c], ord);
+                    if (cc < bc) { bc = cc; best = c; bo = &ord; }
+                }
+                if (bc == 0) break;
+            }
+            const int j = keep[best];
+            const std::vector<int8_t> ord = *bo;
+            std::swap(keep[best], keep.back());
+            keep.pop_back();
+            take(j, ord);
+        }
+        rem.swap(keep);
+    }
+    for (int mi = 0; mi < m; mi++) q.icperm[q.cperm[mi]] = mi;
+    // wavefront count of one gather pass, for diagnostics
+    for (int g = 0; g < m; g += 32) {
+        for (int qq = 0; qq < kw; qq++) {
+            int cnt[32] = {0}, mx = 0;
+            for (int mi = g; mi < std::min(m, g + 32); mi++) {
+                const int j = q.cperm[mi];
+                if (qq < p.length[j]) mx = std::max(mx, ++cnt[bank[p.start[j] + order[mi][qq]]]);
+            }
+            waves += std::max(mx, 1);
+        }
+    }
+    q.bank_wavefronts = waves;
+}
+
+}  // namespace
+
+PackedProblem pack(const HostProblem& p, bool permute_literals) {
     PackedProblem q;
     q.n = p.n;
     q.m = p.m;
@@ -122,17 +228,43 @@ PackedProblem pack(const HostProblem& p) {
     q.nslots = q.srow[q.nslices] * 32;
     q.compact = p.n < 32768 && q.nslots <= 65535;
 
+    // slot of every literal (rank in its variable's public-ordered incidence list)
+    std::vector<int32_t> slot_of(p.storage.size(), 0);
+    {
+        std::vector<int32_t> rank(p.n, 0);
+        for (int j = 0; j < p.m; j++)
+            for (int i = 0; i < p.length[j]; i++) {
+                const int v = q.iperm[std::abs(p.storage[p.start[j] + i]) - 1];
+                slot_of[p.start[j] + i] = (q.srow[v >> 5] + rank[v]++) * 32 + (v & 31);
+            }
+    }
+
+    // literal order inside each internal clause (indices into the public clause)
+    std::vector<std::vector<int8_t>> order;
+    if (q.compact) {
+        schedule_clauses(p, q, permute_literals, order);
+    } else {  // the streamed kernels read no shared-memory banks this way: keep the order
+        q.cperm.resize(p.m);
+        q.icperm.resize(p.m);
+        order.assign(p.m, {});
+        for (int j = 0; j < p.m; j++) {
+            q.cperm[j] = q.icperm[j] = j;
+            for (int i = 0; i < p.length[j]; i++) order[j].push_back((int8_t)i);
+        }
+    }
+
     const uint32_t pad = ((uint32_t)std::min(p.n, 32767) << 16) | (uint32_t)std::min(q.nslots, 65535);
     q.lit.assign((size_t)q.k * q.mp, pad);
-    std::vector<int32_t> rank(p.n, 0);  // next row of each internal variable
-    for (int j = 0; j < p.m; j++) {
-        for (int i = 0; i < p.length[j]; i++) {
-            const int lit = p.storage[p.start[j] + i];
-            const int v = q.iperm[std::abs(lit) - 1];
-            const int slot = (q.srow[v >> 5] + rank[v]++) * 32 + (v & 31);
-            if (q.compact)
-                q.lit[(size_t)i * q.mp + j] =
-                    (lit < 0 ? 0x80000000u : 0u) | ((uint32_t)v << 16) | (uint32_t)slot;
+    if (q.compact) {
+        for (int mi = 0; mi < p.m; mi++) {
+            const int j = q.cperm[mi];
+            for (int qq = 0; qq < p.length[j]; qq++) {
+                const int li = p.start[j] + order[mi][qq];
+                const int lit = p.storage[li];
+                const int v = q.iperm[std::abs(lit) - 1];
+                q.lit[(size_t)qq * q.mp + mi] =
+                    (lit < 0 ? 0x80000000u : 0u) | ((uint32_t)v << 16) | (uint32_t)slot_of[li];
+            }
         }
     }
     return q;

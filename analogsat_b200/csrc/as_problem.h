@@ -27,6 +27,14 @@
 //    nslots, so the kernels store unconditionally.
 //    This "compact" encoding needs N < 32768 and at most 65535 slots; larger
 //    instances are rejected by the shared-memory kernels.
+//  * Clause order: internally, clauses are regrouped so that the 32 clauses a warp
+//    handles together touch 32 different shared-memory banks in each literal slot
+//    (the bank of a literal is its internal variable index mod 32, for both the spin
+//    gather and the contribution store).  cperm[m] = public clause of internal
+//    clause m, icperm is its inverse.  With permute_literals the literals inside a
+//    clause may also be reordered for this (FP32 packing only: FP64 keeps the
+//    reference's product order to stay bit-identical).  The contribution slots
+//    keep the public (clause, literal) order either way.
 #pragma once
 
 #include <cstdint>
@@ -60,9 +68,12 @@ struct PackedProblem {
     std::vector<int32_t> srow;     // [nslices + 1]
     std::vector<int32_t> perm;     // internal -> public variable
     std::vector<int32_t> iperm;    // public -> internal variable
+    std::vector<int32_t> cperm;    // internal -> public clause
+    std::vector<int32_t> icperm;   // public -> internal clause
     int max_degree = 0;
+    long bank_wavefronts = 0;      // shared-memory wavefronts of one gather pass (>= 32-clause groups x k)
 };
 
-PackedProblem pack(const HostProblem& p);
+PackedProblem pack(const HostProblem& p, bool permute_literals);
 
 }  // namespace asb

@@ -85,6 +85,13 @@ int32_t as_problem_get_nmk(const as_problem* p, int32_t* n, int32_t* m, int32_t*
 int32_t as_problem_num_literals(const as_problem* p);
 int32_t as_problem_get_clauses(const as_problem* p, int32_t* literals, int32_t* lengths);
 
+/* Device-layout diagnostics of the packing for `precision` (no reference
+ * counterpart): contribution slots, largest variable degree, shared-memory
+ * wavefronts of one spin-gather pass after bank-aware clause grouping (the ideal is
+ * k * ceil(M/32)), and whether the shared-memory kernels accept the instance. */
+int32_t as_problem_layout_stats(const as_problem* p, int32_t precision, int32_t* nslots,
+                                int32_t* max_degree, int64_t* bank_wavefronts, int32_t* compact);
+
 void as_problem_free(as_problem* p);
 
 /* ---- device primitives (ISat, AnalogSAT/solver/ISat.h:31-87) -------------- */

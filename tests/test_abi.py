@@ -118,3 +118,23 @@ def test_instances_follow_reference_distributions():
     assert abs((l2 > 0).mean() - 0.5) < 0.03
     l3, _, _ = make_instance("fast", 100, 4000, 4, seed=2)
     assert l3.size == 16000 and np.abs(l3).max() <= 100
+
+
+def test_packing_layout_quality():
+    """Degree-sorted SELL slots carry little padding and the bank-aware clause grouping
+    cuts the shared-memory wavefronts of a spin-gather pass well below the natural
+    order (the ideal is k * ceil(M/32))."""
+    from analogsat_b200 import SatProblem, AS_PREC_F32_LOGA, AS_PREC_F64
+    from analogsat_b200.instances import make_instance
+    n, m, k = 1000, 4250, 3
+    lits, lens, _ = make_instance("planted", n, m, k, seed=2000)
+    p = SatProblem.from_arrays(lits, lens)
+    ideal = k * ((m + 31) // 32)
+    s32 = p.layout_stats(AS_PREC_F32_LOGA)
+    s64 = p.layout_stats(AS_PREC_F64)
+    assert s32["compact"] and s64["compact"]
+    assert m * k <= s32["nslots"] <= 1.1 * m * k
+    assert s32["bank_wavefronts"] <= 1.6 * ideal   # literal reordering allowed (FP32)
+    assert s64["bank_wavefronts"] <= 2.2 * ideal   # clause regrouping only (FP64)
+    big = SatProblem.from_arrays(*make_instance("fast", 40000, 200000, 4, seed=1)[:2])
+    assert not big.layout_stats()["compact"]
