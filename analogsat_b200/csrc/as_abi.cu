@@ -8,7 +8,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstddef>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -815,5 +817,144 @@ int32_t as_solver_force_threads(as_solver* s, int32_t threads) {
     s->forced_bt = threads;
     s->groups_dirty = true;
     s->invalidate();
+    return AS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free solve (as_solver_solve_noalloc)
+//
+// For callers that must not allocate device memory once they are running -- for
+// example an application that reserves all of the GPU's memory up front for its own
+// pool, or a fixed-latency loop in which a cudaMalloc (which can synchronise the
+// device) is not allowed.  The per-call scratch of the persistent solve kernel (the
+// work counter, the instance's first-solution flag, the wall-clock deadline and the
+// trajectory tables) lives in the file-scope array below instead of in buffers owned
+// by the solver handle.  The array is part of the library image: every GPU that
+// loads the library holds its AS_NOALLOC_SCRATCH_BYTES until the process exits.
+// Every call shares it; each call re-initialises it, so two calls whose kernels
+// overlap on the GPU (different streams, or different host threads) race.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocFlags = AS_NOALLOC_MAX_PROBLEM_INDEX;
+constexpr size_t kNoAllocHeader = 256;  // work counter + deadline, padded
+constexpr size_t kNoAllocFlagBytes = sizeof(int) * kNoAllocFlags;
+constexpr size_t kNoAllocInstOff = kNoAllocHeader + kNoAllocFlagBytes;
+constexpr size_t kNoAllocStateOff = kNoAllocInstOff + sizeof(int) * AS_NOALLOC_MAX_TRAJ;
+constexpr size_t kNoAllocBytes = kNoAllocStateOff + sizeof(long long) * AS_NOALLOC_MAX_TRAJ;
+static_assert(kNoAllocBytes == AS_NOALLOC_SCRATCH_BYTES, "scratch size documented in the header");
+static_assert(kNoAllocInstOff % 16 == 0 && kNoAllocStateOff % 16 == 0, "scratch alignment");
+static_assert(sizeof(as_unit_result) == sizeof(UnitResult), "as_unit_result mirrors UnitResult");
+static_assert(offsetof(as_unit_result, status) == offsetof(UnitResult, status), "layout");
+static_assert(offsetof(as_unit_result, min_violations) == offsetof(UnitResult, min_viol), "layout");
+
+static __device__ __align__(256) unsigned char as_noalloc_scratch[kNoAllocBytes];
+
+// Device address of the scratch array per device (host code only sees a host-side
+// stand-in for the symbol; the address comes from cudaGetSymbolAddress).
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[256] = {};
+
+int noalloc_scratch_address(int dev, unsigned char** out) {
+    if (dev < 0 || dev >= 256) return fail(AS_ERR_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, as_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(AS_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+    return AS_OK;
+}
+
+// Resets the per-call words (work counter, this instance's flag, deadline) and writes
+// the trajectory tables: trajectory u solves problem pidx from states + u * stride.
+__global__ void noalloc_prepare_kernel(unsigned char* scratch, int pidx, int num_traj,
+                                       long long stride, unsigned long long budget_ns) {
+    int* head = reinterpret_cast<int*>(scratch);
+    unsigned long long* deadline = reinterpret_cast<unsigned long long*>(scratch + 8);
+    int* flags = reinterpret_cast<int*>(scratch + kNoAllocHeader);
+    int* inst = reinterpret_cast<int*>(scratch + kNoAllocInstOff);
+    long long* off = reinterpret_cast<long long*>(scratch + kNoAllocStateOff);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        *head = 0;
+        flags[pidx] = 0;
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        *deadline = t + budget_ns;
+    }
+    for (int u = i; u < num_traj; u += gridDim.x * blockDim.x) {
+        inst[u] = pidx;
+        off[u] = (long long)u * stride;
+    }
+}
+
+}  // namespace
+
+int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num_traj, void* states,
+                                as_unit_result* results, void* stream) {
+    if (!s || !states || !results) return fail(AS_ERR_BAD_INPUT, "as_solver_solve_noalloc: null argument");
+    if (problem_index < 0 || problem_index >= (int)s->problems.size())
+        return fail(AS_ERR_BAD_INPUT, "as_solver_solve_noalloc: problem index out of range");
+    if (problem_index >= AS_NOALLOC_MAX_PROBLEM_INDEX)
+        return fail(AS_ERR_UNSUPPORTED, "as_solver_solve_noalloc: problem index must be < "
+                                        "AS_NOALLOC_MAX_PROBLEM_INDEX (4096)");
+    if (num_traj < 1 || num_traj > AS_NOALLOC_MAX_TRAJ)
+        return fail(AS_ERR_UNSUPPORTED, "as_solver_solve_noalloc: num_traj must be in [1, "
+                                        "AS_NOALLOC_MAX_TRAJ] (65536)");
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    unsigned char* scratch = nullptr;
+    int r = noalloc_scratch_address(s->device, &scratch);
+    if (r) return r;
+
+    const PackedProblem& q = s->problems[problem_index];
+    const Variant* v = nullptr;
+    long best = -1;
+    for (const auto& cand : variants()) {
+        if (!fits(cand, q, s->precision, s->smem_limit)) continue;
+        const long score = (cand.exact ? 0 : 1000) + cand.kmax;
+        if (best < 0 || score < best) { best = score; v = &cand; }
+    }
+    if (!v) return fail(AS_ERR_UNSUPPORTED, "as_solver_solve_noalloc: no launch shape fits the problem");
+    const int bt = s->forced_bt ? s->forced_bt : preferred_bt(q);
+    const size_t smem = solver_smem(*v, q);
+    cudaStream_t st = (cudaStream_t)stream;
+
+    noalloc_prepare_kernel<<<std::max(1, std::min(s->sm_count, (num_traj + 255) / 256)), 256, 0, st>>>(
+        scratch, problem_index, num_traj, (long long)(q.n + q.m),
+        s->wall_budget > 0.0 ? (unsigned long long)(s->wall_budget * 1e9) : 0ull);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("prepare launch: ") + cudaGetErrorString(e));
+    e = cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v->fn, bt, smem);
+    if (e != cudaSuccess || occ < 1) return fail(AS_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
+
+    SolveParams P;
+    P.inst = s->pool.inst.as<DevInstance>();
+    P.unit_inst = reinterpret_cast<const int*>(scratch + kNoAllocInstOff);
+    P.unit_state = reinterpret_cast<const long long*>(scratch + kNoAllocStateOff);
+    P.states = states;
+    P.results = reinterpret_cast<UnitResult*>(results);
+    P.queue_head = reinterpret_cast<int*>(scratch);
+    P.inst_solved = reinterpret_cast<int*>(scratch + kNoAllocHeader);
+    P.best_bits = nullptr;
+    P.unit_bits = nullptr;
+    P.num_units = num_traj;
+    P.maxsteps = s->max_steps;
+    P.batch = s->batch;
+    P.stop_on_first = s->stop_on_first;
+    P.eps = s->eps;
+    P.tmax = s->max_time;
+    P.deadline = s->wall_budget > 0.0 ? reinterpret_cast<const unsigned long long*>(scratch + 8) : nullptr;
+    void* args[] = {&P};
+    e = cudaLaunchKernel((const void*)v->fn, dim3(std::min(num_traj, s->sm_count * occ)), dim3(bt), args,
+                         smem, st);
+    if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("solve launch: ") + cudaGetErrorString(e));
     return AS_OK;
 }

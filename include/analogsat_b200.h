@@ -190,6 +190,49 @@ int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas
  * clause count, at least four).  Used by the autotuner. */
 int32_t as_solver_force_threads(as_solver* s, int32_t threads);
 
+/* ---- allocation-free solve (no counterpart in the reference) --------------
+ * For callers that cannot allocate device memory while they run: an application
+ * that has already reserved the GPU's memory for its own pool, or a fixed-latency
+ * loop where a cudaMalloc (which may synchronise the device) is not allowed.
+ * as_solver_solve_noalloc runs the same persistent solve kernel as
+ * as_solver_solve, but keeps its per-call scratch (work counter, first-solution
+ * flag, wall-clock deadline, trajectory tables) in a static device array inside the
+ * library instead of in buffers owned by the solver handle, and calls no allocation
+ * routine.  The array is AS_NOALLOC_SCRATCH_BYTES on every GPU that loads the
+ * library, held until the process exits.
+ *
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls share the array and each call re-initialises it: calls whose work
+ *    overlaps on the GPU (other streams, other host threads) race.  Serialise them.
+ *  - All num_traj trajectories solve problem `problem_index` of the solver (which
+ *    must be < AS_NOALLOC_MAX_PROBLEM_INDEX); num_traj <= AS_NOALLOC_MAX_TRAJ,
+ *    larger requests fail with AS_ERR_UNSUPPORTED.
+ *  - states: DEVICE array of num_traj public states (N+M values each, float for
+ *    AS_PREC_F32_LOGA solvers, double for AS_PREC_F64), initial states in, final
+ *    states out.  results: DEVICE array of num_traj as_unit_result.
+ *  - The solver's settings apply (epsilon, max time/steps, batch size, wall budget,
+ *    stop-on-first); best-assignment tracking is not available here.
+ *  - Asynchronous on `stream`; results are valid once the stream reaches this point. */
+#define AS_NOALLOC_MAX_TRAJ 65536
+#define AS_NOALLOC_MAX_PROBLEM_INDEX 4096
+#define AS_NOALLOC_SCRATCH_BYTES (256 + 4 * 4096 + 12 * 65536)
+
+typedef struct as_unit_result {
+    double time;            /* integrated analog time */
+    double last_step;       /* last accepted step size */
+    int32_t status;         /* SatResult code */
+    int32_t steps;          /* accepted steps */
+    int32_t attempts;       /* attempted steps */
+    int32_t rhs;            /* RHS evaluations */
+    int32_t violations;     /* unsat clauses at the last check */
+    int32_t min_violations; /* fewest unsat clauses seen at any check */
+    int32_t reserved0, reserved1;
+} as_unit_result;
+
+int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num_traj, void* states,
+                                as_unit_result* results, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
