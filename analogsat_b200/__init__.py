@@ -237,6 +237,10 @@ class SatSolver:
     def ForceThreads(self, threads: int):
         check(self._lib.as_solver_force_threads(self._h, int(threads)))
 
+    def SetStorageMode(self, mode: int):
+        """0 automatic, 1 shared memory only, 2 global storage (per-CTA slab) only."""
+        check(self._lib.as_solver_set_storage_mode(self._h, int(mode)))
+
     # -- states (SatSolver::SetSatState, SatSolver.h:183-192) --
     def SetSatStates(self, problem_index, states, stream=None):
         """states: host array of the concatenated public vectors, or a CUDA tensor

@@ -65,6 +65,7 @@ SIGNATURES = [
     ("as_solver_get_best_assignment", _i32, [_vp, _i32, _vp]),
     ("as_solver_get_launch_shape", _i32, [_vp, _pi32, _pi32, _pi32, _pi32]),
     ("as_solver_force_threads", _i32, [_vp, _i32]),
+    ("as_solver_set_storage_mode", _i32, [_vp, _i32]),
     ("as_solver_solve_noalloc", _i32, [_vp, _i32, _i32, _vp, _vp, _vp]),
 ]
 

@@ -55,7 +55,7 @@ struct DevBuf {
 // Device copy of one or more packed instances in a single pool.
 struct DevicePool {
     int device = -1;
-    DevBuf lit, srow, perm, iperm, icperm, inst;
+    DevBuf lit, litw, slotw, srow, perm, iperm, icperm, inst;
     std::vector<DevInstance> host_inst;
 
     template <typename V>
@@ -67,35 +67,42 @@ struct DevicePool {
     }
 
     int upload(const std::vector<const PackedProblem*>& pk, int dev) {
-        size_t nl = 0, nr = 0, np = 0, nc = 0;
+        size_t nl = 0, nw = 0, nr = 0, np = 0, nc = 0;
         for (auto* q : pk) {
             nl += q->lit.size();
+            nw += q->litw.size();
             nr += q->srow.size();
             np += q->perm.size();
             nc += q->icperm.size();
         }
         AS_CUDA(lit.alloc(std::max<size_t>(nl, 1) * 4));
+        AS_CUDA(litw.alloc(std::max<size_t>(nw, 1) * 4));
+        AS_CUDA(slotw.alloc(std::max<size_t>(nw, 1) * 4));
         AS_CUDA(srow.alloc(std::max<size_t>(nr, 1) * 4));
         AS_CUDA(perm.alloc(std::max<size_t>(np, 1) * 4));
         AS_CUDA(iperm.alloc(std::max<size_t>(np, 1) * 4));
         AS_CUDA(icperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
         host_inst.clear();
-        size_t ol = 0, orr = 0, op = 0, oc = 0;
+        size_t ol = 0, ow = 0, orr = 0, op = 0, oc = 0;
         for (auto* q : pk) {
             DevInstance d;
             d.n = q->n; d.m = q->m; d.k = q->k; d.mp = q->mp; d.nslices = q->nslices;
             d.nslots = q->nslots;
-            d.lit = lit.as<uint32_t>() + ol;
+            d.lit = q->lit.empty() ? nullptr : lit.as<uint32_t>() + ol;
+            d.litw = litw.as<uint32_t>() + ow;
+            d.slotw = slotw.as<uint32_t>() + ow;
             d.srow = srow.as<int32_t>() + orr;
             d.perm = perm.as<int32_t>() + op;
             d.iperm = iperm.as<int32_t>() + op;
             d.icperm = icperm.as<int32_t>() + oc;
             int r;
-            if ((r = put(lit, ol, q->lit)) || (r = put(srow, orr, q->srow)) || (r = put(perm, op, q->perm)) ||
+            if ((r = put(lit, ol, q->lit)) || (r = put(litw, ow, q->litw)) || (r = put(slotw, ow, q->slotw)) ||
+                (r = put(srow, orr, q->srow)) || (r = put(perm, op, q->perm)) ||
                 (r = put(iperm, op, q->iperm)) || (r = put(icperm, oc, q->icperm)))
                 return r;
             ol += q->lit.size();
+            ow += q->litw.size();
             orr += q->srow.size();
             op += q->perm.size();
             oc += q->icperm.size();
@@ -127,18 +134,22 @@ struct Variant {
     int precision;  // AS_PREC_*
     int kmax;
     bool exact;     // clause slots == kmax (no runtime length tests)
+    bool gs;        // global-storage mode (per-CTA slab in global memory, wide literals)
     SolveFn fn;
     size_t bytes_per_value;
 };
 
-#define AS_VARIANT_F32(K, EX) Variant{AS_PREC_F32_LOGA, K, EX, &solve_kernel<float, true, K, EX>, 4}
-#define AS_VARIANT_F64(K, EX) Variant{AS_PREC_F64, K, EX, &solve_kernel<double, false, K, EX>, 8}
+#define AS_VARIANT_F32(K, EX, GS) \
+    Variant{AS_PREC_F32_LOGA, K, EX, GS, &solve_kernel<float, true, K, EX, GS>, 4}
+#define AS_VARIANT_F64(K, EX, GS) \
+    Variant{AS_PREC_F64, K, EX, GS, &solve_kernel<double, false, K, EX, GS>, 8}
 
 const std::vector<Variant>& variants() {
     static const std::vector<Variant> v = {
-        AS_VARIANT_F32(3, true),  AS_VARIANT_F32(4, true),  AS_VARIANT_F32(2, true),
-        AS_VARIANT_F32(16, false), AS_VARIANT_F64(3, true), AS_VARIANT_F64(4, true),
-        AS_VARIANT_F64(16, false),
+        AS_VARIANT_F32(3, true, false),  AS_VARIANT_F32(4, true, false), AS_VARIANT_F32(2, true, false),
+        AS_VARIANT_F32(16, false, false), AS_VARIANT_F64(3, true, false), AS_VARIANT_F64(4, true, false),
+        AS_VARIANT_F64(16, false, false), AS_VARIANT_F32(3, true, true),  AS_VARIANT_F32(4, true, true),
+        AS_VARIANT_F32(16, false, true),  AS_VARIANT_F64(3, true, true),  AS_VARIANT_F64(16, false, true),
     };
     return v;
 }
@@ -147,10 +158,18 @@ size_t solver_smem(const Variant& v, const PackedProblem& q) {
     return solve_smem_values(q.n, q.m, q.nslots) * v.bytes_per_value;
 }
 
+// Shared-memory variants need the compact encoding and the whole trajectory in one
+// SM's shared memory; global-storage variants take any size.
 bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_limit) {
     const bool kok = v.exact ? q.k == v.kmax : q.k <= v.kmax;
-    return q.compact && v.precision == precision && kok && solver_smem(v, q) <= smem_limit;
+    if (v.precision != precision || !kok) return false;
+    if (v.gs) return true;
+    return q.compact && solver_smem(v, q) <= smem_limit;
 }
+
+// Preference among fitting variants: shared memory first, then exact K, then the
+// smallest KMAX.
+long variant_score(const Variant& v) { return (v.gs ? 100000 : 0) + (v.exact ? 0 : 1000) + v.kmax; }
 
 // CTA size: the smallest clause count per thread (at least 4) that keeps the CTA at
 // <= 1024 threads, then the fewest threads for that count (multiple of 32), so the
@@ -177,6 +196,7 @@ struct as_problem {
     HostProblem host;
     PackedProblem packed[2];  // [AS_PREC_F32_LOGA]: literals may be reordered; [AS_PREC_F64]: not
     DevicePool dev[2];        // lazily uploaded for the device primitives
+    DevBuf slab[2];           // per-CTA storage of the global-storage primitives
 
     void pack_all() {
         packed[AS_PREC_F32_LOGA] = pack(host, true);
@@ -201,6 +221,7 @@ struct as_solver {
     int stop_on_first = 0;
     int track_best = 0;
     int forced_bt = 0;
+    int storage_mode = 0;  // 0 automatic, 1 shared memory only, 2 global storage only
 
     // trajectories
     int num_traj = 0;
@@ -209,10 +230,14 @@ struct as_solver {
     std::vector<long long> traj_bits;  // word offset into best_bits
     long long total_values = 0;
     std::vector<int> order;            // launch order -> user trajectory
-    struct Group { int variant, u0, u1, bt; };
+    struct Group {
+        int variant, u0, u1, bt, occ, ctas;
+        size_t smem, slab_off;
+        long long slab_stride;
+    };
     std::vector<Group> groups;
 
-    DevBuf states, results, unit_inst, unit_state, unit_bits, queue, solved, deadline, best_bits;
+    DevBuf states, results, unit_inst, unit_state, unit_bits, queue, solved, deadline, best_bits, slab;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
@@ -323,9 +348,6 @@ namespace {
 
 int ensure_uploaded(as_problem* p, int prec) {
     if (p->host.m == 0 || p->host.k == 0) return fail(AS_ERR_NO_PROBLEM, "SAT problem has not been set");
-    if (!p->packed[prec].compact)
-        return fail(AS_ERR_UNSUPPORTED, "instance too large for the shared-memory kernels "
-                                        "(needs N < 32768 and < 65535 contribution slots)");
     int dev = 0;
     AS_CUDA(cudaGetDevice(&dev));
     if (p->dev[prec].device == dev) return AS_OK;
@@ -333,25 +355,45 @@ int ensure_uploaded(as_problem* p, int prec) {
     return p->dev[prec].upload(v, dev);
 }
 
+// Grid-stride launch of a per-state kernel: the shared-memory form when the state
+// fits one SM, else the global-storage form with a per-CTA slab owned by the problem
+// handle (grown on demand; calls on one handle must not overlap).
+template <typename T, typename OUT>
+int launch_per_state(as_problem* p, int prec, void (*fs)(DevInstance, const T*, OUT*, int, long long, T*, long long),
+                     void (*fg)(DevInstance, const T*, OUT*, int, long long, T*, long long), int bt,
+                     size_t vals, bool compact, const T* x, OUT* out, int ns, long long stride,
+                     cudaStream_t st) {
+    int dev = 0, sms = 0, optin = 0, occ = 0;
+    AS_CUDA(cudaGetDevice(&dev));
+    AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t smem = vals * sizeof(T);
+    if (compact && smem + 1024 <= (size_t)optin) {
+        AS_CUDA(cudaFuncSetAttribute(fs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fs, bt, smem));
+        const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
+        fs<<<grid, bt, smem, st>>>(p->dev[prec].host_inst[0], x, out, ns, stride, (T*)nullptr, 0ll);
+    } else {
+        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fg, bt, 0));
+        const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
+        const long long slab_stride = (long long)((vals + 63) / 64 * 64);
+        AS_CUDA(p->slab[prec].alloc((size_t)grid * slab_stride * sizeof(T)));
+        fg<<<grid, bt, 0, st>>>(p->dev[prec].host_inst[0], x, out, ns, stride, p->slab[prec].as<T>(),
+                                 slab_stride);
+    }
+    AS_CUDA(cudaGetLastError());
+    return AS_OK;
+}
+
 template <typename T, bool LOGA, int KMAX, bool EXACT>
 int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
     constexpr int BT = 512;
     constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
     const auto& q = p->packed[prec];
-    const size_t smem = rhs_smem_values(q.n, q.m, q.nslots) * sizeof(T);
-    auto fn = &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT>;
-    int dev = 0, sms = 0, optin = 0, occ = 0;
-    AS_CUDA(cudaGetDevice(&dev));
-    AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (smem > (size_t)optin)
-        return fail(AS_ERR_UNSUPPORTED, "instance too large for the shared-memory RHS kernel");
-    AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
-    const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
-    fn<<<grid, BT, smem, st>>>(p->dev[prec].host_inst[0], x, d, ns, (long long)(q.n + q.m));
-    AS_CUDA(cudaGetLastError());
-    return AS_OK;
+    return launch_per_state<T, T>(p, prec, &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT, false>,
+                                  &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT, true>, BT,
+                                  rhs_smem_values(q.n, q.m, q.nslots), q.compact, x, d, ns,
+                                  (long long)(q.n + q.m), st);
 }
 
 template <typename T, bool LOGA>
@@ -374,19 +416,10 @@ int launch_viol(as_problem* p, const T* x, int* c, int ns, cudaStream_t st) {
     constexpr int BT = 256;
     constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
     const auto& q = p->packed[prec];
-    const size_t smem = (size_t)((q.n + 1 + 3) & ~3) * sizeof(T);
-    auto fn = &viol_batch_kernel<T, KMAX, EXACT, BT>;
-    int dev = 0, sms = 0, optin = 0, occ = 0;
-    AS_CUDA(cudaGetDevice(&dev));
-    AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (smem > (size_t)optin) return fail(AS_ERR_UNSUPPORTED, "instance too large for the clause-check kernel");
-    AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
-    const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
-    fn<<<grid, BT, smem, st>>>(p->dev[prec].host_inst[0], x, c, ns, (long long)(q.n + q.m));
-    AS_CUDA(cudaGetLastError());
-    return AS_OK;
+    return launch_per_state<T, int>(p, prec, &viol_batch_kernel<T, KMAX, EXACT, BT, false>,
+                                    &viol_batch_kernel<T, KMAX, EXACT, BT, true>, BT,
+                                    (size_t)((q.n + 1 + 3) & ~3), q.compact, x, c, ns,
+                                    (long long)(q.n + q.m), st);
 }
 
 template <typename T>
@@ -557,7 +590,8 @@ int build_groups(as_solver* s) {
         for (int i = 0; i < (int)vs.size(); i++) {
             const auto& v = vs[i];
             if (!fits(v, q, s->precision, s->smem_limit)) continue;
-            const long score = (v.exact ? 0 : 1000) + v.kmax;  // exact first, then smallest KMAX
+            if ((s->storage_mode == 1 && v.gs) || (s->storage_mode == 2 && !v.gs)) continue;
+            const long score = variant_score(v);
             if (best < 0 || score < best) { best = score; pv[p] = i; }
         }
         if (pv[p] < 0)
@@ -572,16 +606,37 @@ int build_groups(as_solver* s) {
         return pi[a] < pi[b];
     });
     s->groups.clear();
+    size_t slab_total = 0;
     for (int u = 0; u < num_traj;) {
-        const int v = pv[pi[s->order[u]]];
+        const int vi = pv[pi[s->order[u]]];
+        const Variant& v = vs[vi];
         int e = u, bt = 64;
-        while (e < num_traj && pv[pi[s->order[e]]] == v) {
-            bt = std::max(bt, preferred_bt(s->problems[pi[s->order[e]]]));
+        size_t vals = 0;
+        while (e < num_traj && pv[pi[s->order[e]]] == vi) {
+            const auto& q = s->problems[pi[s->order[e]]];
+            bt = std::max(bt, preferred_bt(q));
+            vals = std::max(vals, solve_smem_values(q.n, q.m, q.nslots));
             e++;
         }
-        s->groups.push_back({v, u, e, s->forced_bt ? s->forced_bt : bt});
+        as_solver::Group G;
+        G.variant = vi;
+        G.u0 = u;
+        G.u1 = e;
+        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? 512 : bt);
+        G.smem = v.gs ? 0 : vals * v.bytes_per_value;
+        AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem));
+        int occ = 0;
+        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.fn, G.bt, G.smem));
+        if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
+        G.occ = occ;
+        G.ctas = std::min(e - u, s->sm_count * occ);
+        G.slab_stride = v.gs ? (long long)((vals + 63) / 64 * 64) : 0;
+        G.slab_off = slab_total;
+        slab_total += (size_t)G.ctas * (size_t)G.slab_stride * v.bytes_per_value;
+        s->groups.push_back(G);
         u = e;
     }
+    if (slab_total) AS_CUDA(s->slab.alloc(slab_total));
     std::vector<int> ui(num_traj);
     std::vector<long long> us(num_traj), ub(num_traj);
     for (int u = 0; u < num_traj; u++) {
@@ -639,17 +694,8 @@ int record_solve(as_solver* s, cudaStream_t st) {
     for (size_t g = 0; g < s->groups.size(); g++) {
         const auto& G = s->groups[g];
         const Variant& v = vs[G.variant];
-        size_t smem = 0;
-        for (int u = G.u0; u < G.u1; u++) {
-            const auto& q = s->problems[s->traj_problem[s->order[u]]];
-            smem = std::max(smem, solver_smem(v, q));
-        }
-        AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int occ = 0;
-        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.fn, G.bt, smem));
-        if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
-        const int units = G.u1 - G.u0;
-        const int ctas = std::min(units, s->sm_count * occ);
+        const size_t smem = G.smem;
+        const int occ = G.occ, ctas = G.ctas, units = G.u1 - G.u0;
         SolveParams P;
         P.inst = s->pool.inst.as<DevInstance>();
         P.unit_inst = s->unit_inst.as<int>() + G.u0;
@@ -667,6 +713,8 @@ int record_solve(as_solver* s, cudaStream_t st) {
         P.eps = s->eps;
         P.tmax = s->max_time;
         P.deadline = have_deadline ? s->deadline.as<unsigned long long>() : nullptr;
+        P.slab = v.gs ? static_cast<char*>(s->slab.p) + G.slab_off : nullptr;
+        P.slab_stride = G.slab_stride;
         void* args[] = {&P};
         AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(G.bt), args, smem, st));
         s->last_bt = G.bt; s->last_ctas = ctas; s->last_smem = (int)smem; s->last_occ = occ;
@@ -810,6 +858,15 @@ int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas
     return AS_OK;
 }
 
+int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (mode < 0 || mode > 2) return fail(AS_ERR_BAD_INPUT, "storage mode must be 0, 1 or 2");
+    s->storage_mode = mode;
+    s->groups_dirty = true;
+    s->invalidate();
+    return AS_OK;
+}
+
 int32_t as_solver_force_threads(as_solver* s, int32_t threads) {
     if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
     if (threads != 0 && (threads < 32 || threads > 1024 || threads % 32 != 0))
@@ -915,8 +972,8 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
     const Variant* v = nullptr;
     long best = -1;
     for (const auto& cand : variants()) {
-        if (!fits(cand, q, s->precision, s->smem_limit)) continue;
-        const long score = (cand.exact ? 0 : 1000) + cand.kmax;
+        if (cand.gs || !fits(cand, q, s->precision, s->smem_limit)) continue;
+        const long score = variant_score(cand);
         if (best < 0 || score < best) { best = score; v = &cand; }
     }
     if (!v) return fail(AS_ERR_UNSUPPORTED, "as_solver_solve_noalloc: no launch shape fits the problem");
@@ -952,6 +1009,8 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
     P.eps = s->eps;
     P.tmax = s->max_time;
     P.deadline = s->wall_budget > 0.0 ? reinterpret_cast<const unsigned long long*>(scratch + 8) : nullptr;
+    P.slab = nullptr;
+    P.slab_stride = 0;
     void* args[] = {&P};
     e = cudaLaunchKernel((const void*)v->fn, dim3(std::min(num_traj, s->sm_count * occ)), dim3(bt), args,
                          smem, st);

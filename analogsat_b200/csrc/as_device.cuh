@@ -25,7 +25,9 @@ namespace asb {
 // One packed instance in device memory.
 struct DevInstance {
     int n, m, k, mp, nslices, nslots;
-    const uint32_t* lit;   // [k][mp] literal words (var | sign | slot)
+    const uint32_t* lit;    // [k][mp] compact literal words (var | sign | slot), or null
+    const uint32_t* litw;   // [k][mp] wide literal words: sign << 31 | variable
+    const uint32_t* slotw;  // [k][mp] contribution slot of each wide literal
     const int32_t* srow;   // [nslices + 1] SELL row offsets
     const int32_t* perm;    // internal -> public variable
     const int32_t* iperm;   // public -> internal variable
@@ -54,9 +56,6 @@ __device__ __forceinline__ float exp2_fast(float u) {
     return r;
 }
 
-__device__ __forceinline__ uint32_t lit_var(uint32_t w) { return (w >> 16) & 0x7fffu; }
-__device__ __forceinline__ uint32_t lit_slot(uint32_t w) { return w & 0xffffu; }
-__device__ __forceinline__ bool lit_neg(uint32_t w) { return (w >> 31) != 0; }
 
 // Read-only loads of instance data, kept inside the stage loop (hoisting them would
 // cost registers across all six stages; they hit L1).
@@ -71,6 +70,28 @@ __device__ __forceinline__ int32_t ld_ro(const int32_t* p) {
     return v;
 }
 
+// One literal of a clause.  ENC 0: compact word (sign | 15-bit variable | 16-bit
+// slot), one load.  ENC 1: wide words (sign | 31-bit variable, 32-bit slot), two loads,
+// for instances beyond the compact limits.
+template <int ENC> struct Lit;
+template <> struct Lit<0> {
+    uint32_t w;
+    __device__ __forceinline__ void load(const DevInstance& I, int idx) { w = ld_ro(I.lit + idx); }
+    __device__ __forceinline__ uint32_t var() const { return (w >> 16) & 0x7fffu; }
+    __device__ __forceinline__ uint32_t slot() const { return w & 0xffffu; }
+    __device__ __forceinline__ bool neg() const { return (w >> 31) != 0; }
+};
+template <> struct Lit<1> {
+    uint32_t w, s;
+    __device__ __forceinline__ void load(const DevInstance& I, int idx) {
+        w = ld_ro(I.litw + idx);
+        s = ld_ro(I.slotw + idx);
+    }
+    __device__ __forceinline__ uint32_t var() const { return w & 0x7fffffffu; }
+    __device__ __forceinline__ uint32_t slot() const { return s; }
+    __device__ __forceinline__ bool neg() const { return (w >> 31) != 0; }
+};
+
 // Clause phase for one clause m: stores the per-literal spin contributions into cs
 // and returns da_m (du_m in log space).  `am` is a_m in linear space.
 // EXACT: every clause has exactly KMAX slots (shorter clauses are padded with the
@@ -78,20 +99,19 @@ __device__ __forceinline__ int32_t ld_ro(const int32_t* p) {
 // tests are needed; otherwise the runtime length k <= KMAX is honoured.  For
 // k <= 10 the leave-one-out products follow CpuProdWrapper (ascending,
 // left-associated); for k > 10 the generic CalculateAll form (CpuSat.cpp:291-349).
-template <typename T, bool LOGA, int KMAX, bool EXACT>
+template <typename T, bool LOGA, int KMAX, bool EXACT, int ENC>
 __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* __restrict__ sy,
                                           T* __restrict__ cs, T am, T knorm) {
     using A = Arith<T>;
-    uint32_t w[KMAX];
+    Lit<ENC> w[KMAX];
     T f[KMAX];
     T km = knorm;
-    const uint32_t* lp = I.lit + m;
 #pragma unroll
     for (int q = 0; q < KMAX; q++) {
         if (EXACT || q < I.k) {
-            w[q] = ld_ro(lp + q * I.mp);
-            const T s = sy[lit_var(w[q])];
-            f[q] = lit_neg(w[q]) ? A::add(T(1), s) : A::sub(T(1), s);
+            w[q].load(I, q * I.mp + m);
+            const T s = sy[w[q].var()];
+            f[q] = w[q].neg() ? A::add(T(1), s) : A::sub(T(1), s);
             km = A::mul(km, f[q]);
         }
     }
@@ -114,7 +134,7 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
                 }
                 T rr = A::mul(r, prod);
                 rr = rr + rr;
-                cs[lit_slot(w[q])] = lit_neg(w[q]) ? -rr : rr;
+                cs[w[q].slot()] = w[q].neg() ? -rr : rr;
             }
         }
     } else {
@@ -126,7 +146,7 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
                 for (int l = 0; l < KMAX; l++)
                     if (EXACT || l < I.k) temp = A::mul(temp, l == q ? T(1) : f[l]);
                 const T rr = A::mul(A::mul(A::mul(T(2), temp), knorm), am);
-                cs[lit_slot(w[q])] = lit_neg(w[q]) ? -rr : rr;
+                cs[w[q].slot()] = w[q].neg() ? -rr : rr;
             }
         }
     }
@@ -149,15 +169,16 @@ __device__ __forceinline__ T var_phase(const DevInstance& I, int v, const T* __r
 
 // Clause check for clause m against the spins in sy (CpuSat.cpp:136-164): a
 // variable is TRUE when s > 0; the sentinel (s = -1, positive) is FALSE.
-template <int KMAX, bool EXACT, typename T>
+template <int KMAX, bool EXACT, int ENC, typename T>
 __device__ __forceinline__ int clause_violated(const DevInstance& I, int m, const T* sy) {
     bool sat = false;
 #pragma unroll
     for (int q = 0; q < KMAX; q++) {
         if (EXACT || q < I.k) {
-            const uint32_t w = ld_ro(I.lit + q * I.mp + m);
-            const bool t = sy[lit_var(w)] > T(0);
-            sat |= lit_neg(w) ? !t : t;
+            Lit<ENC> w;
+            w.load(I, q * I.mp + m);
+            const bool t = sy[w.var()] > T(0);
+            sat |= w.neg() ? !t : t;
         }
     }
     return sat ? 0 : 1;

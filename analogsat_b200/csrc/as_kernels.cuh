@@ -57,6 +57,8 @@ struct SolveParams {
     double eps;
     double tmax;
     const unsigned long long* deadline;  // %globaltimer deadline (device word); null = none
+    void* slab;                  // global-storage mode: per-CTA trajectory storage
+    long long slab_stride;       // values per CTA slab
 };
 
 // Cash-Karp tableau and NR step controller (AnalogSAT/cpu_sat/CpuRungeKutta.h:72-112).
@@ -156,7 +158,7 @@ __host__ __device__ inline size_t solve_smem_values(int n, int m, int nslots) {
     return 6 * E + (size_t)((n + 1 + 3) & ~3) + (size_t)nslots + 1;
 }
 
-template <typename T, bool LOGA, int KMAX, bool EXACT>
+template <typename T, bool LOGA, int KMAX, bool EXACT, int ENC>
 struct Solver {
     using A = Arith<T>;
     using ET = T;  // error-ratio type (see rk_err_ratio)
@@ -179,7 +181,7 @@ struct Solver {
             T am;
             if constexpr (LOGA) am = exp2_fast(y);
             else am = y;
-            const T d = clause_phase<T, LOGA, KMAX, EXACT>(I, m, sy, cs, am, knorm);
+            const T d = clause_phase<T, LOGA, KMAX, EXACT, ENC>(I, m, sy, cs, am, knorm);
             if constexpr (S == 1) st.K1[e] = d;
             if constexpr (S == 2) st.K2[e] = d;
             if constexpr (S == 3) st.K3[e] = d;
@@ -210,10 +212,15 @@ struct Solver {
 
 // Any block size that is a multiple of 32 and at most 1024 works; the host picks it
 // so that every thread handles about the same number of clauses.
-template <typename T, bool LOGA, int KMAX, bool EXACT>
+// GS = false: the trajectory lives in shared memory (compact literal words).
+// GS = true:  "global storage" mode for instances too large for one SM's shared
+//             memory: the same layout in a per-CTA slab of global memory (L2
+//             resident when the active slabs fit), wide literal words.
+template <typename T, bool LOGA, int KMAX, bool EXACT, bool GS>
 __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
     using A = Arith<T>;
-    using S = Solver<T, LOGA, KMAX, EXACT>;
+    constexpr int ENC = GS ? 1 : 0;
+    using S = Solver<T, LOGA, KMAX, EXACT, ENC>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red_d[34];
     __shared__ int red_i[32];
@@ -229,7 +236,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         const DevInstance I = P.inst[pidx];
         const int n = I.n, E = I.n + I.m;
         const int Ep = (E + 3) & ~3;
-        T* base = reinterpret_cast<T*>(smem_raw);
+        T* base = GS ? reinterpret_cast<T*>(P.slab) + (long long)blockIdx.x * P.slab_stride
+                     : reinterpret_cast<T*>(smem_raw);
         Stages<T> st{base, base + Ep, base + 2 * Ep, base + 3 * Ep, base + 4 * Ep, base + 5 * Ep};
         T* sy = base + 6 * Ep;
         T* cs = sy + ((n + 1 + 3) & ~3);
@@ -310,7 +318,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
             for (int v = tid; v < n; v += nt) sy[v] = st.X[v];
             __syncthreads();
             int cnt = 0;
-            for (int m = tid; m < I.m; m += nt) cnt += clause_violated<KMAX, EXACT>(I, m, sy);
+            for (int m = tid; m < I.m; m += nt) cnt += clause_violated<KMAX, EXACT, ENC>(I, m, sy);
             viol = block_sum(cnt, red_i);
             if (viol < minviol) {
                 minviol = viol;
@@ -371,12 +379,14 @@ __host__ __device__ inline size_t rhs_smem_values(int n, int m, int nslots) {
     return (size_t)((n + 1 + 3) & ~3) + (size_t)((m + 3) & ~3) + (size_t)nslots + 1;
 }
 
-template <typename T, bool LOGA, int KMAX, bool EXACT, int BT>
+template <typename T, bool LOGA, int KMAX, bool EXACT, int BT, bool GS>
 __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* __restrict__ x,
                                                         T* __restrict__ dxdt, int ntraj,
-                                                        long long stride) {
+                                                        long long stride, T* slab,
+                                                        long long slab_stride) {
+    constexpr int ENC = GS ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sy = reinterpret_cast<T*>(smem_raw);
+    T* sy = GS ? slab + (long long)blockIdx.x * slab_stride : reinterpret_cast<T*>(smem_raw);
     T* ab = sy + ((I.n + 1 + 3) & ~3);  // clause weights in internal clause order
     T* cs = ab + ((I.m + 3) & ~3);
     const int tid = threadIdx.x;
@@ -396,7 +406,7 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
             T am;
             if constexpr (LOGA) am = exp2_fast(a);
             else am = a;
-            ab[m] = clause_phase<T, LOGA, KMAX, EXACT>(I, m, sy, cs, am, knorm);
+            ab[m] = clause_phase<T, LOGA, KMAX, EXACT, ENC>(I, m, sy, cs, am, knorm);
         }
         __syncthreads();
         // ds in internal order -> sy (no longer read) -> public order, coalesced
@@ -409,13 +419,15 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
 }
 
 // Exact unsat counts of many states: one CTA per state.
-template <typename T, int KMAX, bool EXACT, int BT>
+template <typename T, int KMAX, bool EXACT, int BT, bool GS>
 __global__ void __launch_bounds__(BT) viol_batch_kernel(DevInstance I, const T* __restrict__ x,
                                                          int* __restrict__ counts, int ntraj,
-                                                         long long stride) {
+                                                         long long stride, T* slab,
+                                                         long long slab_stride) {
+    constexpr int ENC = GS ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int red_i[32];
-    T* sy = reinterpret_cast<T*>(smem_raw);
+    T* sy = GS ? slab + (long long)blockIdx.x * slab_stride : reinterpret_cast<T*>(smem_raw);
     const int tid = threadIdx.x;
     for (int tr = blockIdx.x; tr < ntraj; tr += gridDim.x) {
         const T* X = x + (long long)tr * stride;
@@ -423,7 +435,7 @@ __global__ void __launch_bounds__(BT) viol_batch_kernel(DevInstance I, const T* 
         if (tid == 0) sy[I.n] = T(-1);
         __syncthreads();
         int cnt = 0;
-        for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX, EXACT>(I, m, sy);
+        for (int m = tid; m < I.m; m += BT) cnt += clause_violated<KMAX, EXACT, ENC>(I, m, sy);
         cnt = block_sum(cnt, red_i);
         if (tid == 0) counts[tr] = cnt;
         __syncthreads();

@@ -253,18 +253,21 @@ PackedProblem pack(const HostProblem& p, bool permute_literals) {
         }
     }
 
-    const uint32_t pad = ((uint32_t)std::min(p.n, 32767) << 16) | (uint32_t)std::min(q.nslots, 65535);
-    q.lit.assign((size_t)q.k * q.mp, pad);
-    if (q.compact) {
-        for (int mi = 0; mi < p.m; mi++) {
-            const int j = q.cperm[mi];
-            for (int qq = 0; qq < p.length[j]; qq++) {
-                const int li = p.start[j] + order[mi][qq];
-                const int lit = p.storage[li];
-                const int v = q.iperm[std::abs(lit) - 1];
-                q.lit[(size_t)qq * q.mp + mi] =
-                    (lit < 0 ? 0x80000000u : 0u) | ((uint32_t)v << 16) | (uint32_t)slot_of[li];
-            }
+    const size_t nw = (size_t)q.k * q.mp;
+    q.litw.assign(nw, (uint32_t)p.n);
+    q.slotw.assign(nw, (uint32_t)q.nslots);
+    if (q.compact) q.lit.assign(nw, ((uint32_t)p.n << 16) | (uint32_t)q.nslots);
+    for (int mi = 0; mi < p.m; mi++) {
+        const int j = q.cperm[mi];
+        for (int qq = 0; qq < p.length[j]; qq++) {
+            const int li = p.start[j] + order[mi][qq];
+            const int lit = p.storage[li];
+            const uint32_t v = (uint32_t)q.iperm[std::abs(lit) - 1];
+            const uint32_t neg = lit < 0 ? 0x80000000u : 0u;
+            const size_t idx = (size_t)qq * q.mp + mi;
+            q.litw[idx] = neg | v;
+            q.slotw[idx] = (uint32_t)slot_of[li];
+            if (q.compact) q.lit[idx] = neg | (v << 16) | (uint32_t)slot_of[li];
         }
     }
     return q;

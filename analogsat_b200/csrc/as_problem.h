@@ -25,8 +25,9 @@
 //    the reference's zero padding against its constant FALSE slot
 //    (CpuSat.cpp:214-215), and its contribution lands in the never-read trash slot
 //    nslots, so the kernels store unconditionally.
-//    This "compact" encoding needs N < 32768 and at most 65535 slots; larger
-//    instances are rejected by the shared-memory kernels.
+//    This "compact" encoding needs N < 32768 and at most 65535 slots.  The "wide"
+//    encoding (litw: sign << 31 | variable, slotw: slot) has no such limits and is
+//    used by the global-storage kernels for larger instances.
 //  * Clause order: internally, clauses are regrouped so that the 32 clauses a warp
 //    handles together touch 32 different shared-memory banks in each literal slot
 //    (the bank of a literal is its internal variable index mod 32, for both the spin
@@ -64,7 +65,9 @@ struct PackedProblem {
     int nslices = 0;     // ceil(n / 32)
     int nslots = 0;      // srow[nslices] * 32 (slot nslots is the trash slot)
     bool compact = false;
-    std::vector<uint32_t> lit;     // [k][mp] literal words
+    std::vector<uint32_t> lit;     // [k][mp] compact literal words (empty unless compact)
+    std::vector<uint32_t> litw;    // [k][mp] wide literal words: sign << 31 | internal variable
+    std::vector<uint32_t> slotw;   // [k][mp] contribution slot of each wide literal
     std::vector<int32_t> srow;     // [nslices + 1]
     std::vector<int32_t> perm;     // internal -> public variable
     std::vector<int32_t> iperm;    // public -> internal variable

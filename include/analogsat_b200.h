@@ -189,6 +189,14 @@ int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas
  * the automatic choice (the fewest threads that give every thread about the same
  * clause count, at least four).  Used by the autotuner. */
 int32_t as_solver_force_threads(as_solver* s, int32_t threads);
+/* Where a trajectory lives while it is integrated (no reference counterpart):
+ * AS_STORAGE_AUTO picks shared memory when the instance fits one SM and global
+ * storage (a per-CTA slab in device memory) otherwise; the other two force one.
+ * Solves fail with AS_ERR_UNSUPPORTED when a forced mode cannot hold an instance. */
+#define AS_STORAGE_AUTO 0
+#define AS_STORAGE_SHARED 1
+#define AS_STORAGE_GLOBAL 2
+int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode);
 
 /* ---- allocation-free solve (no counterpart in the reference) --------------
  * For callers that cannot allocate device memory while they run: an application

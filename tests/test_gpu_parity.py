@@ -8,7 +8,7 @@ Tolerances:
     within 1e-9 relative (the controller's pow() may differ from glibc by an ulp).
   * FP32 (log-space a) RHS vs FP64: |d32 - d64| <= 1e-5 * max|d64| per vector.
   * FP32 solver vs an FP64 run of the same integrator over a short horizon:
-    relative state error <= 1e-5.
+    error <= 1e-5 relative to max(|x|, 1) at equal analog time.
 """
 import numpy as np
 import pytest
@@ -160,7 +160,8 @@ def test_solver_f32_short_horizon_error(oracle, golden, tag, nsteps):
     """FP32 state + log-space a against the FP64 solution of the same ODE at the same
     analog time (oracle integrated to the GPU's end time with eps 1e-10).  FP32 noise
     in the error estimate changes the step sequence, so states are compared at equal
-    time, not equal step count.  Bound: 1e-5 relative (floor 1e-2 for near-zero spins)."""
+    time, not equal step count.  Bound: 1e-5 relative to max(|x|, 1), i.e. absolute
+    for spins (|s| <= 1) and relative for clause weights (a >= 1)."""
     from analogsat_b200 import AS_PREC_F32_LOGA
     ic = golden[f"{tag}/traj_ic"]
     s = _solver(golden, tag, AS_PREC_F32_LOGA, 1e-6, nsteps, nsteps)
@@ -172,7 +173,7 @@ def test_solver_f32_short_horizon_error(oracle, golden, tag, nsteps):
     o = oracle.integrate_to(op, ic, r["time"][0], eps=1e-10)
     assert abs(o["time"] - r["time"][0]) <= 1e-12 * r["time"][0]
     x = s.GetSatState(0)
-    err = np.abs(x - o["state"]) / np.maximum(np.abs(o["state"]), 1e-2)
+    err = np.abs(x - o["state"]) / np.maximum(np.abs(o["state"]), 1.0)
     assert err.max() <= 1e-5, err.max()
 
 
