@@ -28,7 +28,7 @@ def sources() -> list[str]:
 def headers() -> list[str]:
     inc = os.path.join(os.path.dirname(HERE), "include")
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    hs += [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith((".h", ".hpp"))]
+    hs += [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
     return hs
 
 

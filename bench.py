@@ -68,6 +68,19 @@ def parse_args():
     return ap.parse_args()
 
 
+def reduce_over_ranks(dist, sums, tmax, device):
+    """Sum `sums` and take the max of `tmax` over all ranks (identity without dist).
+    The replicas exchange nothing else: this is the only collective of the run."""
+    if dist is None:
+        return np.asarray(sums, np.float64), float(tmax)
+    import torch
+    s = torch.tensor(np.asarray(sums, np.float64), device=device)
+    t = torch.tensor([float(tmax)], dtype=torch.float64, device=device)
+    dist.all_reduce(s)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return s.cpu().numpy(), float(t.item())
+
+
 def make_workload(rank: int, instances: int, traj: int):
     from analogsat_b200.instances import make_instance, initial_states
     W = WORKLOAD
@@ -270,15 +283,8 @@ def run_ours(args):
     step_ms = [a.elapsed_time(c) for a, _, c in evs]
     kern_ms = [b.elapsed_time(c) for _, b, c in evs]
     t_total = sum(step_ms) / 1e3
-    t_max = t_total
-    sums = np.array([totals["solved"], totals["rhs"], totals["inst"]], np.float64)
-    if dist is not None:
-        tt = torch.tensor([t_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        ss = torch.tensor(sums, device="cuda")
-        dist.all_reduce(ss)
-        sums = ss.cpu().numpy()
+    sums, t_max = reduce_over_ranks(dist, [totals["solved"], totals["rhs"], totals["inst"]], t_total,
+                                    "cuda")
     solved_all, rhs_all, inst_all = sums
 
     rhs_line = rhs_kernel_bench(A, probs[0], ics_dev, nm, st) if not args.no_rhs_bench else None
@@ -302,13 +308,7 @@ def run_ours(args):
                          else len(set(pidx[r["status"] == 0])))
         barrier()
         t_e = time.perf_counter() - t0
-        if dist is not None:
-            tt = torch.tensor([t_e, e_solved], device="cuda", dtype=torch.float64)
-            t_e_max = torch.tensor([t_e], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t_e_max, op=dist.ReduceOp.MAX)
-            dist.all_reduce(tt)
-            e_solved = float(tt[1].item())
-            t_e = float(t_e_max.item())
+        (e_solved,), t_e = reduce_over_ranks(dist, [e_solved], t_e, "cuda")
         res_bytes = len(pidx) * 48
         e2e = {"value": e_solved / t_e, "unit": "solves/s", "h2d_bytes_per_step": int(ics.nbytes),
                "d2h_bytes_per_step": int(ics.nbytes + res_bytes), "seconds": t_e}
