@@ -21,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libanalogsat_ref.so")
+REFCUDA_SO = os.path.join(HERE, "_ref", "libanalogsat_refcuda.so")
 
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -32,7 +33,7 @@ def build(reference_root: str | None = "/root/reference") -> None:
     """Compile the C restatement, and the reference solver when its sources exist."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if reference_root and os.path.isdir(reference_root):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={reference_root}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "refcuda", f"REF={reference_root}"], check=True)
 
 
 def _flat(clauses):
@@ -283,3 +284,40 @@ class Reference:
         sol = np.zeros(max(p.n, 1), np.int32)
         code = self.L.ref_minisat(p.h, sol.ctypes.data_as(C.c_void_p))
         return code, sol[: p.n]
+
+
+class RefCuda:
+    """The reference's own CUDA path (CudaSat1 + CudaRungeKutta via SatSolver, one
+    instance and one trajectory per solver) built for sm_100a: the plain GPU path."""
+
+    def __init__(self, path: str = REFCUDA_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"reference CUDA comparator not built: {path}")
+        L = C.CDLL(path)
+        L.refcuda_solve_many.restype = C.c_int
+        L.refcuda_solve_many.argtypes = [
+            C.c_int, C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), _i32p, C.c_int, _i32p,
+            _f64p, _i64p, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _i32p, _i32p, _i32p,
+            _f64p, C.POINTER(C.c_double)]
+        self.L = L
+
+    def solve_many(self, problems, prob_idx, ics, precision=1, eps=1e-6, tmax=1e8,
+                   maxsteps=100000, batch=50, wall_budget=0.0):
+        """problems: list of (literals, lengths); unit u solves problems[prob_idx[u]] from ics[u]."""
+        lits = [np.ascontiguousarray(l, np.int32) for l, _ in problems]
+        lens = [np.ascontiguousarray(n, np.int32) for _, n in problems]
+        lp = (C.c_void_p * len(lits))(*[a.ctypes.data for a in lits])
+        np_ = (C.c_void_p * len(lens))(*[a.ctypes.data for a in lens])
+        ms = np.array([len(n) for n in lens], np.int32)
+        prob_idx = np.ascontiguousarray(prob_idx, np.int32)
+        n = len(prob_idx)
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(x, np.float64) for x in ics]))
+        offs = np.zeros(n, np.int64)
+        if n > 1:
+            offs[1:] = np.cumsum([len(x) for x in ics])[:-1]
+        res = np.full(n, -1, np.int32); st = np.zeros(n, np.int32); rh = np.zeros(n, np.int32)
+        tm = np.zeros(n); wall = C.c_double()
+        done = self.L.refcuda_solve_many(precision, len(problems), lp, np_, ms, n, prob_idx, flat, offs,
+                                         eps, tmax, maxsteps, batch, wall_budget, res, st, rh, tm,
+                                         C.byref(wall))
+        return dict(done=done, result=res, steps=st, rhs=rh, time=tm, wall=wall.value)
