@@ -194,14 +194,23 @@ __global__ void stamp_deadline_kernel(unsigned long long* out, unsigned long lon
 // ---------------------------------------------------------------------------
 struct as_problem {
     HostProblem host;
-    PackedProblem packed[2];  // [AS_PREC_F32_LOGA]: literals may be reordered; [AS_PREC_F64]: not
+    // [AS_PREC_F32_LOGA]: literals may be reordered; [AS_PREC_F64]: reference order.
+    // Packed on first use of each precision.
+    PackedProblem packed_[2];
+    bool have_[2] = {false, false};
+    std::mutex mu_;
     DevicePool dev[2];        // lazily uploaded for the device primitives
     DevBuf slab[2];           // per-CTA storage of the global-storage primitives
 
-    void pack_all() {
-        packed[AS_PREC_F32_LOGA] = pack(host, true);
-        packed[AS_PREC_F64] = pack(host, false);
+    const PackedProblem& packed(int prec) {
+        std::lock_guard<std::mutex> lock(mu_);
+        if (!have_[prec]) {
+            packed_[prec] = pack(host, prec == AS_PREC_F32_LOGA);
+            have_[prec] = true;
+        }
+        return packed_[prec];
     }
+    void pack_all() {}
 };
 
 struct as_solver {
@@ -333,7 +342,7 @@ int32_t as_problem_layout_stats(const as_problem* p, int32_t precision, int32_t*
                                 int32_t* max_degree, int64_t* bank_wavefronts, int32_t* compact) {
     if (!p || (precision != AS_PREC_F32_LOGA && precision != AS_PREC_F64))
         return fail(AS_ERR_BAD_INPUT, "as_problem_layout_stats: bad argument");
-    const auto& q = p->packed[precision];
+    const auto& q = const_cast<as_problem*>(p)->packed(precision);
     if (nslots) *nslots = q.nslots;
     if (max_degree) *max_degree = q.max_degree;
     if (bank_wavefronts) *bank_wavefronts = q.bank_wavefronts;
@@ -351,7 +360,7 @@ int ensure_uploaded(as_problem* p, int prec) {
     int dev = 0;
     AS_CUDA(cudaGetDevice(&dev));
     if (p->dev[prec].device == dev) return AS_OK;
-    std::vector<const PackedProblem*> v{&p->packed[prec]};
+    std::vector<const PackedProblem*> v{&p->packed(prec)};
     return p->dev[prec].upload(v, dev);
 }
 
@@ -389,7 +398,7 @@ template <typename T, bool LOGA, int KMAX, bool EXACT>
 int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
     constexpr int BT = 512;
     constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
-    const auto& q = p->packed[prec];
+    const auto& q = p->packed(prec);
     return launch_per_state<T, T>(p, prec, &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT, false>,
                                   &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT, true>, BT,
                                   rhs_smem_values(q.n, q.m, q.nslots), q.compact, x, d, ns,
@@ -404,7 +413,7 @@ int dispatch_rhs(as_problem* p, const T* x, T* d, int ns, void* stream) {
     int r = ensure_uploaded(p, prec);
     if (r) return r;
     cudaStream_t st = (cudaStream_t)stream;
-    const int k = p->packed[prec].k;
+    const int k = p->packed(prec).k;
     if (k == 3) return launch_rhs<T, LOGA, 3, true>(p, x, d, ns, st);
     if (k == 4) return launch_rhs<T, LOGA, 4, true>(p, x, d, ns, st);
     if (k <= 16) return launch_rhs<T, LOGA, 16, false>(p, x, d, ns, st);
@@ -415,7 +424,7 @@ template <typename T, int KMAX, bool EXACT>
 int launch_viol(as_problem* p, const T* x, int* c, int ns, cudaStream_t st) {
     constexpr int BT = 256;
     constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
-    const auto& q = p->packed[prec];
+    const auto& q = p->packed(prec);
     return launch_per_state<T, int>(p, prec, &viol_batch_kernel<T, KMAX, EXACT, BT, false>,
                                     &viol_batch_kernel<T, KMAX, EXACT, BT, true>, BT,
                                     (size_t)((q.n + 1 + 3) & ~3), q.compact, x, c, ns,
@@ -430,7 +439,7 @@ int dispatch_viol(as_problem* p, const T* x, int* c, int ns, void* stream) {
     int r = ensure_uploaded(p, prec);
     if (r) return r;
     cudaStream_t st = (cudaStream_t)stream;
-    const int k = p->packed[prec].k;
+    const int k = p->packed(prec).k;
     if (k == 3) return launch_viol<T, 3, true>(p, x, c, ns, st);
     if (k == 4) return launch_viol<T, 4, true>(p, x, c, ns, st);
     if (k <= 16) return launch_viol<T, 16, false>(p, x, c, ns, st);
@@ -474,7 +483,7 @@ int32_t as_solver_create(const as_problem* const* problems, int32_t num_problems
     int r = current_device(device, &s->device);
     if (r) return r;
     s->precision = precision;
-    for (int i = 0; i < num_problems; i++) s->problems.push_back(problems[i]->packed[precision]);
+    for (int i = 0; i < num_problems; i++) s->problems.push_back(const_cast<as_problem*>(problems[i])->packed(precision));
     std::vector<const PackedProblem*> pk;
     for (auto& q : s->problems) pk.push_back(&q);
     r = s->pool.upload(pk, s->device);

@@ -152,7 +152,7 @@ void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
         for (; i < rem.size() && filled < 32; i++) {
             const int j = rem[i];
             bool placed = false;
-            if (scanned < 4096) {
+            if (scanned < 1024) {
                 scanned++;
                 for (const auto& ord : perms[p.length[j]])
                     if (cost(j, ord) == 0) { take(j, ord); placed = true; break; }

@@ -23,7 +23,6 @@ def make_instance(kind: str, n: int, m: int, k: int, seed: int):
     planted = rng.random(n) < 0.5 if kind == "planted" else None
     unique = kind in ("random", "planted")
     out = np.zeros((0, k), np.int64)
-    seen = set()
     while out.shape[0] < m:
         need = m - out.shape[0]
         B = max(64, int(need * 1.5) + 16)
@@ -37,12 +36,12 @@ def make_instance(kind: str, n: int, m: int, k: int, seed: int):
             sat = np.any(np.where(lits > 0, truth, ~truth), axis=1)
             lits = lits[sat]
         if unique:
-            keep = []
-            for row in map(tuple, lits):
-                if row not in seen:
-                    seen.add(row)
-                    keep.append(row)
-            lits = np.array(keep, np.int64).reshape(-1, k)
+            # keep the first occurrence of every clause, in draw order, across draws
+            allc = np.concatenate([out, lits])
+            _, first = np.unique(allc, axis=0, return_index=True)
+            keep = np.zeros(len(allc), bool)
+            keep[first] = True
+            lits = allc[len(out):][keep[len(out):]]
         out = np.concatenate([out, lits[:need]])
     return (out.reshape(-1).astype(np.int32), np.full(m, k, np.int32), planted)
 

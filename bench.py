@@ -63,6 +63,12 @@ def parse_args():
     ap.add_argument("--no-rhs-bench", action="store_true")
     ap.add_argument("--all-trajectories", action="store_true",
                     help="run every trajectory to its own SatResult (no early exit per instance)")
+    ap.add_argument("--workload", default="planted1000", choices=["planted1000", "uneven", "maxsat"],
+                    help="planted1000: the headline configuration; uneven: 512 planted instances "
+                         "N~U{100..5000}, alpha~U(3.8,4.26), 64 trajectories each, one graph-captured "
+                         "launch; maxsat: one random 4-SAT N=1e5, M=1e6 instance, 32 trajectories, "
+                         "minimise unsat over --maxsat-seconds")
+    ap.add_argument("--maxsat-seconds", type=float, default=60.0)
     ap.add_argument("--max-steps", type=int, default=WORKLOAD["maxsteps"],
                     help="per-trajectory step cap (profiling runs use a small one)")
     return ap.parse_args()
@@ -423,10 +429,95 @@ def verify_solutions(solver, probs_raw, pidx, r, nm):
         raise SystemExit(f"{bad} reported solutions failed the exact clause check")
 
 
+def run_uneven(args):
+    """512 planted 3-SAT instances of uneven size, 64 trajectories each, first solution per
+    instance stops the rest; the whole batch is one graph-captured solve call (shared-
+    memory launch group for instances that fit one SM, global-storage group for the rest)."""
+    import torch
+    import analogsat_b200 as A
+    from analogsat_b200.instances import make_instance, initial_states
+    rng = np.random.default_rng(3000)
+    P, T = 512, 64
+    ns = rng.integers(100, 5001, size=P)
+    alphas = rng.uniform(3.8, 4.26, size=P)
+    raw, sizes = [], []
+    t0 = time.perf_counter()
+    for i in range(P):
+        n = int(ns[i]); m = int(np.floor(alphas[i] * n))
+        lits, lens, _ = make_instance("planted", n, m, 3, seed=3000 + i)
+        raw.append((lits, lens)); sizes.append((n, m))
+    probs = [A.SatProblem.from_arrays(l, c) for l, c in raw]
+    s = A.SatSolver(probs)
+    s.SetEpsilon(1e-6); s.SetBatchSize(50); s.SetMaxSteps(args.max_steps); s.SetMaxTime(1e8)
+    s.SetStopOnFirst(True)
+    pidx = np.repeat(np.arange(P), T).astype(np.int32)
+    X = np.concatenate([initial_states(n, m, T, seed=40_000 + i, dtype=np.float32)
+                        for i, (n, m) in enumerate(sizes)])
+    setup = time.perf_counter() - t0
+    s.SetSatStates(pidx, X)
+    s.Solve()  # warm-up: builds launch groups, captures the graph
+    shape = s.launch_shape()
+    walls, solved, rhs = [], 0, 0
+    for _ in range(args.steps):
+        s.SetSatStates(pidx, X)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        s.Solve()
+        walls.append(time.perf_counter() - t1)
+        r = s.results()
+        solved += len(set(pidx[r["status"] == 0]))
+        rhs += int(r["rhs"].sum())
+    wall = sum(walls)
+    small = sum(1 for p in probs if p.layout_stats()["compact"] and p.n <= 1200)
+    print(json.dumps({"workload": "uneven-planted-3sat-512-inst-N100-5000-x64-traj", "instances": P,
+                      "trajectories_per_instance": T, "solves/s": solved / wall,
+                      "instances_solved_fraction": solved / (P * args.steps),
+                      "rhs_evals_per_s": rhs / wall, "ms_per_solve_call": 1000 * wall / args.steps,
+                      "setup_s": setup, "last_group_launch_shape": shape,
+                      "instances_N_le_1200": small}), flush=True)
+
+
+def run_maxsat(args):
+    """One random 4-SAT instance N=1e5, M=1e6 (alpha 10, unsatisfiable w.h.p.), 32
+    trajectories, minimise the unsat-clause count within a wall-clock budget; the best
+    assignment of every trajectory is kept on device and re-counted exactly here."""
+    import analogsat_b200 as A
+    from analogsat_b200.instances import make_instance, initial_states
+    n, m, k, T = 100_000, 1_000_000, 4, 32
+    lits, lens, _ = make_instance("fast", n, m, k, seed=5000)
+    p = A.SatProblem.from_arrays(lits, lens)
+    s = A.SatSolver([p])
+    s.SetEpsilon(1e-6); s.SetBatchSize(10); s.SetMaxSteps(10 ** 9); s.SetMaxTime(1e30)
+    s.SetTrackBest(True)
+    s.SetWallBudget(args.maxsat_seconds)
+    X = initial_states(n, m, T, seed=50_000, dtype=np.float32)
+    s.SetSatStates(np.zeros(T, np.int32), X)
+    t0 = time.perf_counter()
+    s.Solve()
+    wall = time.perf_counter() - t0
+    r = s.results()
+    c = lits.reshape(-1, k)
+    v = np.abs(c) - 1
+    exact = []
+    for t in range(T):
+        best = s.GetBestAssignment(t)
+        exact.append(int((~np.where(c > 0, best[v], ~best[v]).any(axis=1)).sum()))
+    assert exact == list(r["min_violations"]), "device min-unsat disagrees with the host recount"
+    print(json.dumps({"workload": "maxsat-random-4sat-N1e5-M1e6-x32-traj", "wall_s": wall,
+                      "budget_s": args.maxsat_seconds, "min_unsat": int(min(exact)),
+                      "median_min_unsat": float(np.median(exact)), "steps_median": float(np.median(r["steps"])),
+                      "rhs_evals_per_s": float(r["rhs"].sum()) / wall,
+                      "launch_shape": s.launch_shape()}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "uneven":
+        run_uneven(args)
+    elif args.workload == "maxsat":
+        run_maxsat(args)
     else:
         run_ours(args)
 
