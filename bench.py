@@ -356,7 +356,10 @@ def run_ours(args):
         "gpu_launches": args.steps * len(solver_groups(solver)),
         "roofline": {"bound": "hbm", "kernel": "solve_kernel", "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     "traffic": None,
+                     # ncu dram__bytes_read+write of one solve_kernel launch over 148
+                     # trajectories (profiles/solve_kernel_planted3sat_N1000_M4250.md):
+                     # 3.31 MB, i.e. 22.4 KB per trajectory, scaled to this launch
+                     "traffic": 3.31e6 / 148 * len(pidx),
                      "note": "achieved = RHS evals x 8(N+M)+4KM bytes / kernel time; state, "
                              "stages and contributions stay on chip (shared memory), so DRAM "
                              "traffic is far below the algorithmic bytes"},
@@ -407,9 +410,12 @@ def rhs_kernel_bench(A, problem, ics_dev, nm, st, reps=10):
     # algorithmic bytes: state in + derivative out, and the instance's literal stream once
     # per launch (T_share = all B states of the launch)
     bytes_per_launch = B * 8 * nm + 4 * W["k"] * W["m"]
+    # traffic: ncu dram__bytes_read + dram__bytes_write of one launch of this exact
+    # configuration (profiles/rhs_batch_kernel_16384_states_N1000_M4250.md)
     return {"bound": "hbm", "kernel": "rhs_batch_kernel", "states_per_launch": B,
             "ms_per_launch": ms, "achieved": bytes_per_launch / (ms / 1e3) / 1e9, "unit": "GB/s",
-            "bytes_per_launch": bytes_per_launch, "traffic": None}
+            "bytes_per_launch": bytes_per_launch,
+            "traffic": 641.86e6 if B == 16384 else None}
 
 
 def solver_groups(solver):
@@ -452,7 +458,7 @@ def run_uneven(args):
     s.SetStopOnFirst(True)
     pidx = np.repeat(np.arange(P), T).astype(np.int32)
     X = np.concatenate([initial_states(n, m, T, seed=40_000 + i, dtype=np.float32)
-                        for i, (n, m) in enumerate(sizes)])
+                        for i, (n, m) in enumerate(sizes)], axis=None)
     setup = time.perf_counter() - t0
     s.SetSatStates(pidx, X)
     s.Solve()  # warm-up: builds launch groups, captures the graph
