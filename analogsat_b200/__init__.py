@@ -321,6 +321,28 @@ class SatSolver:
                                                       bits.ctypes.data_as(C.c_void_p)))
         return ((bits[np.arange(n) // 32] >> (np.arange(n) % 32).astype(np.uint32)) & 1).astype(bool)
 
+    def Adjoint(self, t_end: float, weights=None, max_steps: int = 4096) -> dict:
+        """Gradients of L = sum_m w_m a_m(T) K_m(T)^2 w.r.t. x(0) and w for every
+        trajectory (see as_solver_adjoint); x(0) is the current state buffer."""
+        nt = len(self._traj_problem)
+        ms = [self._nm[p][1] for p in self._traj_problem]
+        total = int(sum(sum(self._nm[p]) for p in self._traj_problem))
+        loss = np.zeros(nt); gx = np.zeros(total); gw = np.zeros(max(sum(ms), 1))
+        ns = np.zeros(nt, np.int32)
+        hs = np.zeros((nt, max_steps))
+        wp = None
+        if weights is not None:
+            weights = np.ascontiguousarray(weights, np.float64)
+            if weights.size != sum(ms):
+                raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "weights: M values per trajectory")
+            wp = weights.ctypes.data_as(C.c_void_p)
+        check(self._lib.as_solver_adjoint(self._h, float(t_end), int(max_steps), wp,
+                                          loss.ctypes.data_as(C.c_void_p), gx.ctypes.data_as(C.c_void_p),
+                                          gw.ctypes.data_as(C.c_void_p), ns.ctypes.data_as(C.c_void_p),
+                                          hs.ctypes.data_as(C.c_void_p)))
+        return dict(loss=loss, grad_x0=gx, grad_w=gw[: sum(ms)], nsteps=ns,
+                    step_sizes=[hs[t, : ns[t]].copy() for t in range(nt)])
+
     def launch_shape(self) -> dict:
         a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
         check(self._lib.as_solver_get_launch_shape(self._h, C.byref(a), C.byref(b), C.byref(c),

@@ -1026,3 +1026,154 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
     if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("solve launch: ") + cudaGetErrorString(e));
     return AS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Adjoint (gradients of the final potential)
+// ---------------------------------------------------------------------------
+#include "as_adjoint.cuh"
+
+namespace {
+
+using AdjFn = void (*)(AdjointParams);
+
+struct AdjVariant {
+    int precision, kmax;
+    bool exact;
+    AdjFn fwd, bwd;
+    size_t bytes;
+};
+
+#define AS_ADJ(T, P, K, EX) \
+    AdjVariant{P, K, EX, &adj_forward_kernel<T, K, EX>, &adj_backward_kernel<T, K, EX>, sizeof(T)}
+
+const std::vector<AdjVariant>& adj_variants() {
+    static const std::vector<AdjVariant> v = {
+        AS_ADJ(float, AS_PREC_F32_LOGA, 3, true),  AS_ADJ(float, AS_PREC_F32_LOGA, 16, false),
+        AS_ADJ(double, AS_PREC_F64, 3, true),      AS_ADJ(double, AS_PREC_F64, 16, false),
+    };
+    return v;
+}
+
+}  // namespace
+
+int32_t as_solver_adjoint(as_solver* s, double t_end, int32_t max_steps, const double* weights, double* loss,
+                          double* grad_x0, double* grad_w, int32_t* nsteps, double* step_sizes) {
+    if (!s || !loss || !grad_x0 || !grad_w) return fail(AS_ERR_BAD_INPUT, "as_solver_adjoint: null argument");
+    if (!(t_end > 0.0) || max_steps < 1) return fail(AS_ERR_BAD_INPUT, "as_solver_adjoint: need t_end > 0, max_steps >= 1");
+    if (s->num_traj <= 0) return fail(AS_ERR_NO_PROBLEM, "no trajectories set (as_solver_set_states_*)");
+    AS_CUDA(cudaSetDevice(s->device));
+    const int nt = s->num_traj;
+    // one launch shape for all trajectories: the largest instance decides
+    const AdjVariant* av = nullptr;
+    size_t vals = 0;
+    int bt = 64;
+    for (int t = 0; t < nt; t++) {
+        const auto& q = s->problems[s->traj_problem[t]];
+        if (!q.compact) return fail(AS_ERR_UNSUPPORTED, "adjoint: instance beyond the compact encoding");
+        vals = std::max(vals, adjoint_smem_values(q.n, q.m, q.nslots));
+        bt = std::max(bt, preferred_bt(q));
+    }
+    for (const auto& v : adj_variants()) {
+        bool ok = v.precision == s->precision;
+        for (int t = 0; ok && t < nt; t++) {
+            const int k = s->problems[s->traj_problem[t]].k;
+            ok = v.exact ? k == v.kmax : k <= v.kmax;
+        }
+        if (ok) { av = &v; break; }
+    }
+    if (!av) return fail(AS_ERR_UNSUPPORTED, "adjoint: clause length > 16");
+    const size_t smem = vals * av->bytes;
+    if (smem > s->smem_limit) return fail(AS_ERR_UNSUPPORTED, "adjoint: instance too large for one SM");
+
+    std::vector<int> ui(nt);
+    std::vector<long long> us(nt), uw(nt);
+    long long wtot = 0;
+    for (int t = 0; t < nt; t++) {
+        ui[t] = s->traj_problem[t];
+        us[t] = s->traj_off[t];
+        uw[t] = wtot;
+        wtot += s->problems[s->traj_problem[t]].m;
+    }
+    DevBuf d_ui, d_us, d_uw, d_w, d_hs, d_ns, d_loss, d_gx, d_gw, d_uc, d_ck;
+    const size_t vb = av->bytes;
+    AS_CUDA(d_ui.alloc(sizeof(int) * nt));
+    AS_CUDA(d_us.alloc(sizeof(long long) * nt));
+    AS_CUDA(d_uw.alloc(sizeof(long long) * nt));
+    AS_CUDA(d_hs.alloc(sizeof(double) * (size_t)nt * max_steps));
+    AS_CUDA(d_ns.alloc(sizeof(int) * (nt + 2)));
+    AS_CUDA(d_loss.alloc(sizeof(double) * nt));
+    AS_CUDA(d_gx.alloc(vb * (size_t)s->total_values));
+    AS_CUDA(d_gw.alloc(sizeof(double) * (size_t)std::max<long long>(wtot, 1)));
+    AS_CUDA(cudaMemcpy(d_ui.p, ui.data(), sizeof(int) * nt, cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(d_us.p, us.data(), sizeof(long long) * nt, cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(d_uw.p, uw.data(), sizeof(long long) * nt, cudaMemcpyHostToDevice));
+    if (weights) {
+        AS_CUDA(d_w.alloc(sizeof(double) * (size_t)std::max<long long>(wtot, 1)));
+        AS_CUDA(cudaMemcpy(d_w.p, weights, sizeof(double) * wtot, cudaMemcpyHostToDevice));
+    }
+    AS_CUDA(cudaMemset(d_ns.p, 0, sizeof(int) * (nt + 2)));
+
+    AdjointParams P;
+    P.inst = s->pool.inst.as<DevInstance>();
+    P.unit_inst = d_ui.as<int>();
+    P.unit_state = d_us.as<long long>();
+    P.unit_wofs = d_uw.as<long long>();
+    P.x0 = s->states.p;
+    P.weights = weights ? d_w.as<double>() : nullptr;
+    P.hs = d_hs.as<double>();
+    P.nsteps = d_ns.as<int>();
+    P.ckpt = nullptr;
+    P.unit_ckpt = nullptr;
+    P.loss = d_loss.as<double>();
+    P.grad_x0 = d_gx.p;
+    P.grad_w = d_gw.as<double>();
+    P.num_units = nt;
+    P.max_steps = max_steps;
+    P.eps = s->eps;
+    P.t_end = t_end;
+
+    auto launch = [&](AdjFn fn) -> int {
+        AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 0;
+        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, bt, smem));
+        if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "adjoint launch shape does not fit on an SM");
+        void* args[] = {&P};
+        AS_CUDA(cudaLaunchKernel((const void*)fn, dim3(std::min(nt, s->sm_count * occ)), dim3(bt), args, smem,
+                                 s->stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+        return AS_OK;
+    };
+    int r = launch(av->fwd);
+    if (r) return r;
+    std::vector<int> ns(nt);
+    AS_CUDA(cudaMemcpy(ns.data(), d_ns.p, sizeof(int) * nt, cudaMemcpyDeviceToHost));
+    std::vector<long long> uc(nt);
+    long long ctot = 0;
+    for (int t = 0; t < nt; t++) {
+        if (ns[t] < 0)
+            return fail(AS_ERR_UNSUPPORTED, ns[t] == -1 ? "adjoint: more than max_steps steps to reach t_end"
+                                                        : "adjoint: step size underflow");
+        uc[t] = ctot;
+        ctot += (long long)ns[t] * (s->problems[s->traj_problem[t]].n + s->problems[s->traj_problem[t]].m);
+    }
+    AS_CUDA(d_uc.alloc(sizeof(long long) * nt));
+    AS_CUDA(d_ck.alloc(vb * (size_t)std::max<long long>(ctot, 1)));
+    AS_CUDA(cudaMemcpy(d_uc.p, uc.data(), sizeof(long long) * nt, cudaMemcpyHostToDevice));
+    P.ckpt = d_ck.p;
+    P.unit_ckpt = d_uc.as<long long>();
+    r = launch(av->bwd);
+    if (r) return r;
+    AS_CUDA(cudaMemcpy(loss, d_loss.p, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    AS_CUDA(cudaMemcpy(grad_w, d_gw.p, sizeof(double) * wtot, cudaMemcpyDeviceToHost));
+    if (vb == 8) {
+        AS_CUDA(cudaMemcpy(grad_x0, d_gx.p, 8 * (size_t)s->total_values, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp((size_t)s->total_values);
+        AS_CUDA(cudaMemcpy(tmp.data(), d_gx.p, 4 * tmp.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < tmp.size(); i++) grad_x0[i] = tmp[i];
+    }
+    if (nsteps) std::copy(ns.begin(), ns.end(), nsteps);
+    if (step_sizes)
+        AS_CUDA(cudaMemcpy(step_sizes, d_hs.p, sizeof(double) * (size_t)nt * max_steps, cudaMemcpyDeviceToHost));
+    return AS_OK;
+}

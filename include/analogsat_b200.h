@@ -198,6 +198,22 @@ int32_t as_solver_force_threads(as_solver* s, int32_t threads);
 #define AS_STORAGE_GLOBAL 2
 int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode);
 
+/* ---- gradients (no counterpart in the reference: it has no differentiation) --
+ * Weighted CTDS: a_m -> w_m a_m in the potential and the spin equation
+ * (ds_i = sum_m 2 w_m a_m c_mi K_mi K_m, da_m = a_m K_m^2; w = 1 is the reference
+ * ODE) and L = V(x(T)) = sum_m w_m a_m(T) K_m(s(T))^2.  For every trajectory set with
+ * as_solver_set_states_* (the state buffer's current contents are x(0), a linear), the
+ * adaptive RK45 controller runs to t_end (last step clamped), its accepted step sizes
+ * are frozen, and the discrete adjoint of that fixed-step map gives dL/dx(0) and
+ * dL/dw.  weights: NULL (all 1) or, per trajectory, M_p values in public clause order,
+ * concatenated; grad_w has the same shape; grad_x0 the shape of the states (FP64);
+ * loss and nsteps one value per trajectory; step_sizes (may be NULL) receives the
+ * frozen step sizes, max_steps slots per trajectory.  FP32 solvers compute in FP32
+ * with linear a, FP64 solvers in FP64.  Instances must fit one SM's shared memory;
+ * AS_ERR_UNSUPPORTED if a trajectory needs more than max_steps steps. */
+int32_t as_solver_adjoint(as_solver* s, double t_end, int32_t max_steps, const double* weights, double* loss,
+                          double* grad_x0, double* grad_w, int32_t* nsteps, double* step_sizes);
+
 /* ---- allocation-free solve (no counterpart in the reference) --------------
  * For callers that cannot allocate device memory while they run: an application
  * that has already reserved the GPU's memory for its own pool, or a fixed-latency

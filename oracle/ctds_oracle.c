@@ -376,3 +376,219 @@ double orc_potential(const orc_problem* p, const double* x, const double* w) {
     }
     return v;
 }
+
+/* ------------------------------------------------------------------------------------
+ * Differentiation (no reference counterpart: the reference has no gradients).
+ * Weighted CTDS: a_m -> w_m a_m in the potential and in the spin equation,
+ *   ds_i = sum_m 2 w_m a_m c_mi K_mi K_m,   da_m = a_m K_m^2,
+ *   L    = V(x(T)) = sum_m w_m a_m(T) K_m(s(T))^2      (w = 1 is the reference ODE).
+ * The adaptive controller runs once (forward, last step clamped to end at T) and its
+ * accepted step sizes are then frozen: L is a smooth function of (s(0), a(0), w)
+ * through the fixed-step Cash-Karp map, and the discrete adjoint below is its exact
+ * gradient (checked against central finite differences in tests/test_oracle.py).
+ * State vectors here are public-layout [s_1..s_N, a_1..a_M], a linear.
+ * ------------------------------------------------------------------------------------ */
+
+static void clause_vals(const orc_problem* p, const double* x, int j, double* f, int* v, double* c) {
+    int q;
+    for (q = 0; q < p->k; q++) {
+        int idx = p->C[(size_t)j * p->k + q];
+        if (idx == 0) { f[q] = 2.0; v[q] = -1; c[q] = 1.0; continue; }
+        v[q] = abs(idx) - 1;
+        c[q] = idx < 0 ? -1.0 : 1.0;
+        f[q] = 1.0 - c[q] * x[v[q]];
+    }
+}
+
+static double prod_except(const double* f, int k, int a, int b) {
+    double r = 1.0;
+    int l;
+    for (l = 0; l < k; l++)
+        if (l != a && l != b) r *= f[l];
+    return r;
+}
+
+/* f(x; w) */
+static void wrhs(const orc_problem* p, const double* x, const double* w, double* d) {
+    const int n = p->n, m = p->m, k = p->k;
+    double f[64], c[64];
+    int v[64], j, q;
+    memset(d, 0, sizeof(double) * (size_t)(n + m));
+    for (j = 0; j < m; j++) {
+        double K, a = x[n + j], wj = w ? w[j] : 1.0;
+        clause_vals(p, x, j, f, v, c);
+        K = p->knorm * prod_except(f, k, -1, -1);
+        d[n + j] = a * K * K;
+        for (q = 0; q < k; q++)
+            if (v[q] >= 0) d[v[q]] += 2.0 * wj * a * c[q] * (p->knorm * prod_except(f, k, q, -1)) * K;
+    }
+}
+
+/* J(x)^T u and the w-gradient contribution g_w += (df/dw)^T u. */
+static void wvjp(const orc_problem* p, const double* x, const double* w, const double* u, double* out,
+                 double* gw) {
+    const int n = p->n, m = p->m, k = p->k;
+    double f[64], c[64], Kq[64];
+    int v[64], j, q, r;
+    memset(out, 0, sizeof(double) * (size_t)(n + m));
+    for (j = 0; j < m; j++) {
+        const double a = x[n + j], wj = w ? w[j] : 1.0, ua = u[n + j];
+        double K, S = 0.0;
+        clause_vals(p, x, j, f, v, c);
+        K = p->knorm * prod_except(f, k, -1, -1);
+        for (q = 0; q < k; q++) Kq[q] = p->knorm * prod_except(f, k, q, -1);
+        for (q = 0; q < k; q++)
+            if (v[q] >= 0) S += u[v[q]] * c[q] * Kq[q];
+        /* d/da_m: sum_q u_q 2 w c_q K_q K + ua K^2 ;  d/dw_m: sum_q u_q 2 a c_q K_q K */
+        out[n + j] = 2.0 * wj * S * K + ua * K * K;
+        if (gw) gw[j] += 2.0 * a * S * K;
+        /* d/ds_r: -2 c_r [ w a sum_q u_q c_q (K_qr K [q!=r] + K_q K_r) + ua a K K_r ] */
+        for (r = 0; r < k; r++) {
+            double t = 0.0;
+            if (v[r] < 0) continue;
+            for (q = 0; q < k; q++) {
+                double term;
+                if (v[q] < 0) continue;
+                term = Kq[q] * Kq[r];
+                if (q != r) term += p->knorm * prod_except(f, k, q, r) * K;
+                t += u[v[q]] * c[q] * term;
+            }
+            out[v[r]] += -2.0 * c[r] * (wj * a * t + ua * a * K * Kq[r]);
+        }
+    }
+}
+
+static double wpotential(const orc_problem* p, const double* x, const double* w) {
+    return orc_potential(p, x, w);
+}
+
+static const double CK_B[7][6] = {
+    {0}, {0}, {B21}, {B31, B32}, {B41, B42, B43}, {B51, B52, B53, B54}, {B61, B62, B63, B64, B65}};
+static const double CK_C[7] = {0, C1, 0.0, C3, C4, 0.0, C6};
+
+/* One fixed-step Cash-Karp step: x <- x + h sum c_j k_j (k's kept in K[1..6]). */
+static void ck_fixed(const orc_problem* p, double* x, const double* w, double h, double* K[7], double* y) {
+    const size_t E = (size_t)(p->n + p->m);
+    int s, l;
+    size_t i;
+    for (s = 1; s <= 6; s++) {
+        for (i = 0; i < E; i++) {
+            double acc = 0.0;
+            for (l = 1; l < s; l++) acc += CK_B[s][l - 1] * K[l][i];
+            y[i] = x[i] + h * acc;
+        }
+        wrhs(p, y, w, K[s]);
+    }
+    for (i = 0; i < E; i++) {
+        double acc = 0.0;
+        for (s = 1; s <= 6; s++) acc += CK_C[s] * K[s][i];
+        x[i] += h * acc;
+    }
+}
+
+/* Forward adaptive run to t_end (last step clamped), recording accepted step sizes.
+ * Returns the number of steps (or -1 if more than maxsteps). */
+int orc_record_steps(const orc_problem* p, const double* ic, double eps, double t_end, int maxsteps,
+                     double* hs) {
+    rk_t rk;
+    int s = 0;
+    double* x = (double*)malloc(sizeof(double) * (size_t)(p->n + p->m + 1));
+    rk_init(&rk, p, eps, 0);
+    load_ic(p, ic, x, 0);
+    while (rk.time < t_end) {
+        if (s >= maxsteps) { s = -1; break; }
+        if (rk.time + rk.hnext > t_end) rk.hnext = t_end - rk.time;
+        if (!rk_step(&rk, x)) { s = -1; break; }
+        hs[s++] = rk.hdid;
+    }
+    rk_free(&rk);
+    free(x);
+    return s;
+}
+
+/* L(x0, w) through the fixed step sequence hs[0..nsteps). */
+double orc_fixed_loss(const orc_problem* p, const double* x0, const double* w, const double* hs, int nsteps,
+                      double* x_final) {
+    const size_t E = (size_t)(p->n + p->m);
+    double *x = (double*)malloc(sizeof(double) * E * 8), *K[7], *y, L;
+    int s;
+    for (s = 1; s <= 6; s++) K[s] = x + E * (size_t)s;
+    y = x + E * 7;
+    memcpy(x, x0, sizeof(double) * E);
+    for (s = 0; s < nsteps; s++) ck_fixed(p, x, w, hs[s], K, y);
+    L = wpotential(p, x, w);
+    if (x_final) memcpy(x_final, x, sizeof(double) * E);
+    free(x);
+    return L;
+}
+
+/* Discrete adjoint of orc_fixed_loss: g_x0 = dL/dx0 (public layout), g_w = dL/dw. */
+double orc_adjoint(const orc_problem* p, const double* x0, const double* w, const double* hs, int nsteps,
+                   double* g_x0, double* g_w) {
+    const size_t E = (size_t)(p->n + p->m);
+    const int n = p->n, m = p->m;
+    double *ck = (double*)malloc(sizeof(double) * E * (size_t)(nsteps + 1));
+    double *buf = (double*)malloc(sizeof(double) * E * 20), *K[7], *sig[7], *y, *lam, *rho, *tmp, L;
+    int s, j, i2, l;
+    size_t i;
+    for (s = 1; s <= 6; s++) K[s] = buf + E * (size_t)(s - 1);
+    for (s = 1; s <= 6; s++) sig[s] = buf + E * (size_t)(5 + s);
+    y = buf + E * 12; lam = buf + E * 13; rho = buf + E * 14; tmp = buf + E * 15;
+    /* forward with checkpoints */
+    memcpy(ck, x0, sizeof(double) * E);
+    for (s = 0; s < nsteps; s++) {
+        memcpy(ck + E * (size_t)(s + 1), ck + E * (size_t)s, sizeof(double) * E);
+        ck_fixed(p, ck + E * (size_t)(s + 1), w, hs[s], K, y);
+    }
+    {
+        const double* xT = ck + E * (size_t)nsteps;
+        L = wpotential(p, xT, w);
+        /* dL/dx(T): spins -ds (weighted RHS), weights w K^2; dL/dw = a K^2 */
+        wrhs(p, xT, w, tmp);
+        for (i = 0; i < (size_t)n; i++) lam[i] = -tmp[i];
+        for (j = 0; j < m; j++) {
+            const double a = xT[n + j];
+            const double Kk2 = a > 0 ? tmp[n + j] / a : 0.0; /* K^2 = (a K^2) / a */
+            double f[64], c[64], KK;
+            int v[64];
+            clause_vals(p, xT, j, f, v, c);
+            KK = p->knorm * prod_except(f, p->k, -1, -1);
+            (void)Kk2;
+            lam[n + j] = (w ? w[j] : 1.0) * KK * KK;
+            if (g_w) g_w[j] = a * KK * KK;
+        }
+    }
+    /* backward over steps */
+    for (s = nsteps - 1; s >= 0; s--) {
+        const double h = hs[s];
+        const double* xs = ck + E * (size_t)s;
+        /* recompute stage derivatives k1..k5 */
+        for (j = 1; j <= 5; j++) {
+            for (i = 0; i < E; i++) {
+                double acc = 0.0;
+                for (l = 1; l < j; l++) acc += CK_B[j][l - 1] * K[l][i];
+                y[i] = xs[i] + h * acc;
+            }
+            wrhs(p, y, w, K[j]);
+        }
+        for (j = 6; j >= 1; j--) {
+            for (i = 0; i < E; i++) {
+                double acc = CK_C[j] * lam[i];
+                for (i2 = j + 1; i2 <= 6; i2++) acc += CK_B[i2][j - 1] * sig[i2][i];
+                rho[i] = h * acc;
+            }
+            for (i = 0; i < E; i++) {
+                double acc = 0.0;
+                for (l = 1; l < j; l++) acc += CK_B[j][l - 1] * K[l][i];
+                y[i] = xs[i] + h * acc;
+            }
+            wvjp(p, y, w, rho, sig[j], g_w);
+        }
+        for (i = 0; i < E; i++)
+            lam[i] += sig[1][i] + sig[2][i] + sig[3][i] + sig[4][i] + sig[5][i] + sig[6][i];
+    }
+    memcpy(g_x0, lam, sizeof(double) * E);
+    free(ck);
+    free(buf);
+    return L;
+}

@@ -51,6 +51,16 @@ int orc_integrate_to(const orc_problem* p, const double* ic, double eps, double 
 /* Potential V = sum_m w_m a_m K_m^2 of a public state (a linear). */
 double orc_potential(const orc_problem* p, const double* x, const double* w);
 
+/* Differentiation (weighted ODE, see ctds_oracle.c): record the accepted step sizes of
+ * an adaptive run to t_end, evaluate L = V(x(T)) through that frozen step sequence,
+ * and its discrete adjoint (gradients w.r.t. x0 = [s(0), a(0)] and w). */
+int orc_record_steps(const orc_problem* p, const double* ic, double eps, double t_end, int maxsteps,
+                     double* hs);
+double orc_fixed_loss(const orc_problem* p, const double* x0, const double* w, const double* hs, int nsteps,
+                      double* x_final);
+double orc_adjoint(const orc_problem* p, const double* x0, const double* w, const double* hs, int nsteps,
+                   double* g_x0, double* g_w);
+
 #ifdef __cplusplus
 }
 #endif

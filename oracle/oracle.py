@@ -68,6 +68,12 @@ class Oracle:
                                        _f64p, C.POINTER(C.c_double)]
         L.orc_potential.restype = C.c_double
         L.orc_potential.argtypes = [C.c_void_p, _f64p, C.c_void_p]
+        L.orc_record_steps.restype = C.c_int
+        L.orc_record_steps.argtypes = [C.c_void_p, _f64p, C.c_double, C.c_double, C.c_int, _f64p]
+        L.orc_fixed_loss.restype = C.c_double
+        L.orc_fixed_loss.argtypes = [C.c_void_p, _f64p, C.c_void_p, _f64p, C.c_int, C.c_void_p]
+        L.orc_adjoint.restype = C.c_double
+        L.orc_adjoint.argtypes = [C.c_void_p, _f64p, C.c_void_p, _f64p, C.c_int, _f64p, _f64p]
         self.L = L
 
     class Problem:
@@ -125,6 +131,33 @@ class Oracle:
         steps = self.L.orc_integrate_to(p.h, np.ascontiguousarray(ic, np.float64), eps, t_end,
                                         int(logspace), maxsteps, out, C.byref(t))
         return dict(state=out, time=t.value, steps=steps)
+
+    def record_steps(self, p, ic, t_end, eps=1e-6, maxsteps=100000):
+        hs = np.zeros(maxsteps)
+        n = self.L.orc_record_steps(p.h, np.ascontiguousarray(ic, np.float64), eps, t_end, maxsteps, hs)
+        if n < 0:
+            raise RuntimeError("step recording failed (underflow or too many steps)")
+        return hs[:n].copy()
+
+    @staticmethod
+    def _wptr(w):
+        if w is None:
+            return None, None
+        w = np.ascontiguousarray(w, np.float64)
+        return w, w.ctypes.data_as(C.c_void_p)
+
+    def fixed_loss(self, p, x0, hs, w=None):
+        w, wp = self._wptr(w)
+        return self.L.orc_fixed_loss(p.h, np.ascontiguousarray(x0, np.float64), wp,
+                                     np.ascontiguousarray(hs, np.float64), len(hs), None)
+
+    def adjoint(self, p, x0, hs, w=None):
+        w, wp = self._wptr(w)
+        gx = np.zeros(p.n + p.m)
+        gw = np.zeros(p.m)
+        L = self.L.orc_adjoint(p.h, np.ascontiguousarray(x0, np.float64), wp,
+                               np.ascontiguousarray(hs, np.float64), len(hs), gx, gw)
+        return L, gx, gw
 
     def potential(self, p, x, w=None):
         wp = None

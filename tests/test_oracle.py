@@ -125,3 +125,28 @@ def test_oracle_vs_live_reference(oracle):
         a = R.steps(rp, x, 1e-6, 50)
         b = oracle.steps(op, x, 1e-6, 50)
         assert np.array_equal(a["states"], b["states"]) and np.array_equal(a["h"], b["h"])
+
+
+def test_oracle_adjoint_matches_central_differences(oracle):
+    """The differentiation configuration's shape (random 3-SAT N=200, M=850, T=5):
+    the FP64 discrete adjoint of the frozen-step RK45 map against central finite
+    differences (h = 1e-4) along 64 random unit directions of x(0) and of w."""
+    from analogsat_b200.instances import make_instance, initial_states
+    lits, lens, _ = make_instance("random", 200, 850, 3, seed=4)
+    p = oracle.problem(lits, lens)
+    x0 = initial_states(200, 850, 1, seed=2)[0]
+    hs = oracle.record_steps(p, x0, 5.0)
+    rng = np.random.default_rng(0)
+    w = rng.uniform(0.5, 1.5, 850)
+    L, gx, gw = oracle.adjoint(p, x0, hs, w)
+    assert np.isclose(L, oracle.fixed_loss(p, x0, hs, w), rtol=1e-14)
+    eh = 1e-4
+    errs = []
+    for _ in range(64):
+        d = rng.normal(size=x0.shape); d /= np.linalg.norm(d)
+        fd = (oracle.fixed_loss(p, x0 + eh * d, hs, w) - oracle.fixed_loss(p, x0 - eh * d, hs, w)) / (2 * eh)
+        errs.append(abs(fd - gx @ d) / max(abs(fd), 1e-12))
+        dw = rng.normal(size=w.shape); dw /= np.linalg.norm(dw)
+        fd = (oracle.fixed_loss(p, x0, hs, w + eh * dw) - oracle.fixed_loss(p, x0, hs, w - eh * dw)) / (2 * eh)
+        errs.append(abs(fd - gw @ dw) / max(abs(fd), 1e-12))
+    assert np.median(errs) < 1e-7 and max(errs) < 1e-4
