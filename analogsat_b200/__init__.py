@@ -237,6 +237,10 @@ class SatSolver:
     def ForceThreads(self, threads: int):
         check(self._lib.as_solver_force_threads(self._h, int(threads)))
 
+    def SetClusterSize(self, ctas: int):
+        """CTAs per trajectory in global-storage mode: 0 automatic, 1, 4 or 8."""
+        check(self._lib.as_solver_set_cluster_size(self._h, int(ctas)))
+
     def SetStorageMode(self, mode: int):
         """0 automatic, 1 shared memory only, 2 global storage (per-CTA slab) only."""
         check(self._lib.as_solver_set_storage_mode(self._h, int(mode)))

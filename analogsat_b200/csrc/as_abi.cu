@@ -134,22 +134,25 @@ struct Variant {
     int precision;  // AS_PREC_*
     int kmax;
     bool exact;     // clause slots == kmax (no runtime length tests)
-    bool gs;        // global-storage mode (per-CTA slab in global memory, wide literals)
+    bool gs;        // global-storage mode (slab in global memory per trajectory, wide literals)
+    int cl;         // CTAs per trajectory (thread-block cluster), global storage only
     SolveFn fn;
     size_t bytes_per_value;
 };
 
-#define AS_VARIANT_F32(K, EX, GS) \
-    Variant{AS_PREC_F32_LOGA, K, EX, GS, &solve_kernel<float, true, K, EX, GS>, 4}
-#define AS_VARIANT_F64(K, EX, GS) \
-    Variant{AS_PREC_F64, K, EX, GS, &solve_kernel<double, false, K, EX, GS>, 8}
+#define AS_VARIANT_F32(K, EX, GS, CL) \
+    Variant{AS_PREC_F32_LOGA, K, EX, GS, CL, &solve_kernel<float, true, K, EX, GS, CL>, 4}
+#define AS_VARIANT_F64(K, EX, GS, CL) \
+    Variant{AS_PREC_F64, K, EX, GS, CL, &solve_kernel<double, false, K, EX, GS, CL>, 8}
 
 const std::vector<Variant>& variants() {
     static const std::vector<Variant> v = {
-        AS_VARIANT_F32(3, true, false),  AS_VARIANT_F32(4, true, false), AS_VARIANT_F32(2, true, false),
-        AS_VARIANT_F32(16, false, false), AS_VARIANT_F64(3, true, false), AS_VARIANT_F64(4, true, false),
-        AS_VARIANT_F64(16, false, false), AS_VARIANT_F32(3, true, true),  AS_VARIANT_F32(4, true, true),
-        AS_VARIANT_F32(16, false, true),  AS_VARIANT_F64(3, true, true),  AS_VARIANT_F64(16, false, true),
+        AS_VARIANT_F32(3, true, false, 1),  AS_VARIANT_F32(4, true, false, 1), AS_VARIANT_F32(2, true, false, 1),
+        AS_VARIANT_F32(16, false, false, 1), AS_VARIANT_F64(3, true, false, 1), AS_VARIANT_F64(4, true, false, 1),
+        AS_VARIANT_F64(16, false, false, 1), AS_VARIANT_F32(3, true, true, 1),  AS_VARIANT_F32(4, true, true, 1),
+        AS_VARIANT_F32(16, false, true, 1),  AS_VARIANT_F64(3, true, true, 1),  AS_VARIANT_F64(16, false, true, 1),
+        AS_VARIANT_F32(3, true, true, 4),    AS_VARIANT_F32(4, true, true, 4),  AS_VARIANT_F32(3, true, true, 8),
+        AS_VARIANT_F32(4, true, true, 8),
     };
     return v;
 }
@@ -169,7 +172,9 @@ bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_l
 
 // Preference among fitting variants: shared memory first, then exact K, then the
 // smallest KMAX.
-long variant_score(const Variant& v) { return (v.gs ? 100000 : 0) + (v.exact ? 0 : 1000) + v.kmax; }
+long variant_score(const Variant& v) {
+    return (v.gs ? 100000 : 0) + (v.cl > 1 ? 10000 * v.cl : 0) + (v.exact ? 0 : 1000) + v.kmax;
+}
 
 // CTA size: the smallest clause count per thread (at least 4) that keeps the CTA at
 // <= 1024 threads, then the fewest threads for that count (multiple of 32), so the
@@ -230,6 +235,7 @@ struct as_solver {
     int stop_on_first = 0;
     int track_best = 0;
     int forced_bt = 0;
+    int forced_cl = 0;     // CTAs per trajectory in global-storage mode (0 = automatic)
     int storage_mode = 0;  // 0 automatic, 1 shared memory only, 2 global storage only
 
     // trajectories
@@ -606,6 +612,29 @@ int build_groups(as_solver* s) {
         if (pv[p] < 0)
             return fail(AS_ERR_UNSUPPORTED, "no compiled launch shape fits problem " + std::to_string(p));
     }
+    // global-storage problems with few trajectories: spread each trajectory over a
+    // cluster of CTAs so that all trajectories run at once on the whole GPU
+    {
+        std::vector<int> per_problem(np, 0);
+        for (int t = 0; t < num_traj; t++) per_problem[s->traj_problem[t]]++;
+        long gs_units = 0;
+        for (int p = 0; p < np; p++)
+            if (vs[pv[p]].gs) gs_units += per_problem[p];
+        int want_cl = 1;
+        if (s->forced_cl) want_cl = s->forced_cl;
+        else
+            while (want_cl < 8 && gs_units > 0 && gs_units * want_cl * 2 <= s->sm_count) want_cl *= 2;
+        if (want_cl > 1 && !s->forced_bt) {
+            for (int p = 0; p < np; p++) {
+                const Variant& cur = vs[pv[p]];
+                if (!cur.gs) continue;
+                for (int i = 0; i < (int)vs.size(); i++)
+                    if (vs[i].gs && vs[i].cl == want_cl && vs[i].precision == cur.precision &&
+                        vs[i].kmax == cur.kmax && vs[i].exact == cur.exact)
+                        pv[p] = i;
+            }
+        }
+    }
     const auto& pi = s->traj_problem;
     s->order.resize(num_traj);
     for (int t = 0; t < num_traj; t++) s->order[t] = t;
@@ -631,17 +660,36 @@ int build_groups(as_solver* s) {
         G.variant = vi;
         G.u0 = u;
         G.u1 = e;
-        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? 512 : bt);
+        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : 512) : bt);
         G.smem = v.gs ? 0 : vals * v.bytes_per_value;
         AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem));
         int occ = 0;
-        AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.fn, G.bt, G.smem));
-        if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
-        G.occ = occ;
-        G.ctas = std::min(e - u, s->sm_count * occ);
+        if (v.cl > 1) {
+            AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr;
+            attr.id = cudaLaunchAttributeClusterDimension;
+            attr.val.clusterDim.x = v.cl;
+            attr.val.clusterDim.y = 1;
+            attr.val.clusterDim.z = 1;
+            cfg.gridDim = dim3(v.cl * std::max(1, e - u));
+            cfg.blockDim = dim3(G.bt);
+            cfg.dynamicSmemBytes = G.smem;
+            cfg.attrs = &attr;
+            cfg.numAttrs = 1;
+            AS_CUDA(cudaOccupancyMaxActiveClusters(&occ, (const void*)v.fn, &cfg));
+            if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "cluster launch shape does not fit");
+            G.occ = occ;
+            G.ctas = std::min(e - u, occ) * v.cl;  // clusters resident at once x CTAs per cluster
+        } else {
+            AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v.fn, G.bt, G.smem));
+            if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "launch shape does not fit on an SM");
+            G.occ = occ;
+            G.ctas = std::min(e - u, s->sm_count * occ);
+        }
         G.slab_stride = v.gs ? (long long)((vals + 63) / 64 * 64) : 0;
         G.slab_off = slab_total;
-        slab_total += (size_t)G.ctas * (size_t)G.slab_stride * v.bytes_per_value;
+        slab_total += (size_t)(G.ctas / v.cl) * (size_t)G.slab_stride * v.bytes_per_value;
         s->groups.push_back(G);
         u = e;
     }
@@ -725,7 +773,23 @@ int record_solve(as_solver* s, cudaStream_t st) {
         P.slab = v.gs ? static_cast<char*>(s->slab.p) + G.slab_off : nullptr;
         P.slab_stride = G.slab_stride;
         void* args[] = {&P};
-        AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(G.bt), args, smem, st));
+        if (v.cl > 1) {
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute attr;
+            attr.id = cudaLaunchAttributeClusterDimension;
+            attr.val.clusterDim.x = v.cl;
+            attr.val.clusterDim.y = 1;
+            attr.val.clusterDim.z = 1;
+            cfg.gridDim = dim3(ctas);
+            cfg.blockDim = dim3(G.bt);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = st;
+            cfg.attrs = &attr;
+            cfg.numAttrs = 1;
+            AS_CUDA(cudaLaunchKernelExC(&cfg, (const void*)v.fn, args));
+        } else {
+            AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(G.bt), args, smem, st));
+        }
         s->last_bt = G.bt; s->last_ctas = ctas; s->last_smem = (int)smem; s->last_occ = occ;
     }
     return AS_OK;
@@ -871,6 +935,16 @@ int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode) {
     if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
     if (mode < 0 || mode > 2) return fail(AS_ERR_BAD_INPUT, "storage mode must be 0, 1 or 2");
     s->storage_mode = mode;
+    s->groups_dirty = true;
+    s->invalidate();
+    return AS_OK;
+}
+
+int32_t as_solver_set_cluster_size(as_solver* s, int32_t ctas) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (!(ctas == 0 || ctas == 1 || ctas == 4 || ctas == 8))
+        return fail(AS_ERR_BAD_INPUT, "cluster size must be 0 (automatic), 1, 4 or 8");
+    s->forced_cl = ctas;
     s->groups_dirty = true;
     s->invalidate();
     return AS_OK;

@@ -17,6 +17,7 @@
 // bit-identical to CpuSat<double>.  Layouts are documented in as_problem.h.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -198,10 +199,48 @@ __device__ __forceinline__ int block_sum(int v, int* red) {
     return s;
 }
 
-// Block max (FP64) whose result is post-processed by thread 0: fn(max) is broadcast
-// to every thread through red[32]; fn may publish more values in red[33...].
-template <typename F>
-__device__ __forceinline__ double block_max_then(double v, double* red, F&& fn) {
+// ---- thread groups: one CTA, or a thread-block cluster of CL CTAs cooperating on one
+// trajectory (global-storage mode).  Group-wide barriers are __syncthreads or the
+// cluster barrier (release/acquire at cluster scope, which orders the global-memory
+// slab accesses of all CTAs); values decided by one thread are published to every
+// CTA's shared memory through distributed shared memory.
+template <int CL>
+struct Grp {
+    int rank, gtid, gnt;
+    __device__ __forceinline__ Grp() {
+        if constexpr (CL == 1) {
+            rank = 0;
+        } else {
+            rank = (int)cooperative_groups::this_cluster().block_rank();
+        }
+        gtid = rank * (int)blockDim.x + (int)threadIdx.x;
+        gnt = CL * (int)blockDim.x;
+    }
+    __device__ __forceinline__ void sync() const {
+        if constexpr (CL == 1) __syncthreads();
+        else cooperative_groups::this_cluster().sync();
+    }
+    // Group thread 0 publishes v into `slot` (a __shared__ variable) of every CTA.
+    template <typename V>
+    __device__ __forceinline__ V bcast(V* slot, V v) const {
+        if (gtid == 0) {
+            if constexpr (CL == 1) {
+                *slot = v;
+            } else {
+                auto cl = cooperative_groups::this_cluster();
+                for (int r = 0; r < CL; r++) *cl.map_shared_rank(slot, r) = v;
+            }
+        }
+        sync();
+        return *slot;
+    }
+};
+
+// Group-wide max (FP64) post-processed by one thread: fn(max) is broadcast to every
+// thread.  red: 35 doubles of shared memory per CTA -- [0,32) warp partials, [32] the
+// CTA partial, [33] the result; fn may publish more values in red[34].
+template <int CL, typename F>
+__device__ __forceinline__ double group_max_then(const Grp<CL>& g, double v, double* red, F&& fn) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -211,10 +250,49 @@ __device__ __forceinline__ double block_max_then(double v, double* red, F&& fn) 
     if (threadIdx.x == 0) {
         double m = red[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = fmax(m, red[w]);
-        red[32] = fn(m);
+        red[32] = m;
+    }
+    if constexpr (CL > 1) {
+        g.sync();
+        if (threadIdx.x == 0) {
+            auto cl = cooperative_groups::this_cluster();
+            double m = red[32];
+            for (int r = 0; r < CL; r++) m = fmax(m, *cl.map_shared_rank(red + 32, r));
+            red[33] = fn(m);
+        }
+    } else {
+        if (threadIdx.x == 0) red[33] = fn(red[32]);
     }
     __syncthreads();
-    return red[32];
+    return red[33];
+}
+
+// Group-wide integer sum (red: 33 ints per CTA).
+template <int CL>
+__device__ __forceinline__ int group_sum(const Grp<CL>& g, int v, int* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    int s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+    if constexpr (CL > 1) {
+        if (threadIdx.x == 0) red[32] = s;
+        g.sync();
+        auto cl = cooperative_groups::this_cluster();
+        s = 0;
+        for (int r = 0; r < CL; r++) s += *cl.map_shared_rank(red + 32, r);
+        g.sync();  // red[32] of every CTA may be rewritten after this point
+    }
+    return s;
+}
+
+// Block max (FP64) whose result is post-processed by thread 0 (single-CTA kernels).
+template <typename F>
+__device__ __forceinline__ double block_max_then(double v, double* red, F&& fn) {
+    return group_max_then<1>(Grp<1>(), v, red, fn);
 }
 
 }  // namespace asb

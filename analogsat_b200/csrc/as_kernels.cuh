@@ -158,7 +158,7 @@ __host__ __device__ inline size_t solve_smem_values(int n, int m, int nslots) {
     return 6 * E + (size_t)((n + 1 + 3) & ~3) + (size_t)nslots + 1;
 }
 
-template <typename T, bool LOGA, int KMAX, bool EXACT, int ENC>
+template <typename T, bool LOGA, int KMAX, bool EXACT, int ENC, int CL>
 struct Solver {
     using A = Arith<T>;
     using ET = T;  // error-ratio type (see rk_err_ratio)
@@ -167,13 +167,13 @@ struct Solver {
     // stage vectors; the derivative lands in K_S, or for S == 6 is consumed at once
     // into xnew (stored in K2, dead after the stage-6 input) and the error norm.
     template <int S>
-    static __device__ __forceinline__ void eval(const DevInstance& I, T* sy, T* cs, T knorm,
+    static __device__ __forceinline__ void eval(const Grp<CL>& g, const DevInstance& I, T* sy, T* cs, T knorm,
                                                 const Stages<T>& st, T hT, T h0T, ET& errmax) {
-        const int tid = threadIdx.x, nt = blockDim.x;
+        const int tid = g.gtid, nt = g.gnt;
         const int n = I.n;
         for (int v = tid; v < n; v += nt)
             sy[v] = stage_in<S>(st.X[v], st.K1[v], st.K2[v], st.K3[v], st.K4[v], st.K5[v], hT);
-        __syncthreads();
+        g.sync();
         for (int m = tid; m < I.m; m += nt) {
             const int e = n + m;
             const T x = st.X[e];
@@ -193,7 +193,7 @@ struct Solver {
                 st.K2[e] = rk_new<T>(x, k1, k3, k4, d, hT);
             }
         }
-        __syncthreads();
+        g.sync();
         for (int v = tid; v < n; v += nt) {
             const T d = var_phase<T>(I, v, cs);
             if constexpr (S == 1) st.K1[v] = d;
@@ -214,29 +214,33 @@ struct Solver {
 // so that every thread handles about the same number of clauses.
 // GS = false: the trajectory lives in shared memory (compact literal words).
 // GS = true:  "global storage" mode for instances too large for one SM's shared
-//             memory: the same layout in a per-CTA slab of global memory (L2
-//             resident when the active slabs fit), wide literal words.
-template <typename T, bool LOGA, int KMAX, bool EXACT, bool GS>
+//             memory: the same layout in a slab of global memory per trajectory in
+//             flight (L2 resident when the active slabs fit), wide literal words.
+// CL > 1 (global storage only): a thread-block cluster of CL CTAs on different SMs
+//             works on one trajectory, synchronised by cluster barriers, so a few
+//             very large trajectories still occupy the whole GPU.
+template <typename T, bool LOGA, int KMAX, bool EXACT, bool GS, int CL>
 __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
+    static_assert(CL == 1 || GS, "clusters share a trajectory through global memory");
     using A = Arith<T>;
     constexpr int ENC = GS ? 1 : 0;
-    using S = Solver<T, LOGA, KMAX, EXACT, ENC>;
+    using S = Solver<T, LOGA, KMAX, EXACT, ENC, CL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[34];
-    __shared__ int red_i[32];
+    __shared__ double red_d[35];
+    __shared__ int red_i[33];
     __shared__ int s_unit, s_flag;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const Grp<CL> g;
+    const int tid = g.gtid, nt = g.gnt;
+    const long long slot = blockIdx.x / CL;  // trajectory slot of this CTA (or cluster)
 
     while (true) {
-        if (tid == 0) s_unit = atomicAdd(P.queue_head, 1);
-        __syncthreads();
-        const int u = s_unit;
+        const int u = g.bcast(&s_unit, tid == 0 ? atomicAdd(P.queue_head, 1) : 0);
         if (u >= P.num_units) break;
         const int pidx = P.unit_inst[u];
         const DevInstance I = P.inst[pidx];
         const int n = I.n, E = I.n + I.m;
         const int Ep = (E + 3) & ~3;
-        T* base = GS ? reinterpret_cast<T*>(P.slab) + (long long)blockIdx.x * P.slab_stride
+        T* base = GS ? reinterpret_cast<T*>(P.slab) + slot * P.slab_stride
                      : reinterpret_cast<T*>(smem_raw);
         Stages<T> st{base, base + Ep, base + 2 * Ep, base + 3 * Ep, base + 4 * Ep, base + 5 * Ep};
         T* sy = base + 6 * Ep;
@@ -260,9 +264,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         int status = SAT_UNKNOWN;
 
         // an instance already solved by another trajectory (stop_on_first) is skipped
-        if (tid == 0) s_flag = P.stop_on_first ? (atomicAdd(P.inst_solved + pidx, 0) != 0) : 0;
-        __syncthreads();
-        if (s_flag) status = SAT_ODE_INTERRUPTED;
+        const int skip = g.bcast(&s_flag, tid == 0 && P.stop_on_first ? (atomicAdd(P.inst_solved + pidx, 0) != 0 ? 1 : 0) : 0);
+        if (skip) status = SAT_ODE_INTERRUPTED;
 
         while (status == SAT_UNKNOWN && t < P.tmax && steps < P.maxsteps) {
             bool underflow = false;
@@ -270,7 +273,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
             for (int b = 0; b < P.batch; b++) {
                 // ---- CpuRungeKutta::Step, count = 1 ----
                 T dummy = T(0);
-                S::template eval<1>(I, sy, cs, knorm, st, T(0), T(0), dummy);
+                S::template eval<1>(g, I, sy, cs, knorm, st, T(0), T(0), dummy);
                 rhs++;
                 const double h0 = hnext;
                 const T h0T = (T)h0;
@@ -278,16 +281,16 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
                 while (true) {
                     const T hT = (T)h;
                     T em = T(0);
-                    S::template eval<2>(I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<3>(I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<4>(I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<5>(I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<6>(I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<2>(g, I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<3>(g, I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<4>(g, I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<5>(g, I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<6>(g, I, sy, cs, knorm, st, hT, h0T, em);
                     rhs += 5;
                     attempts++;
                     // step-size control (CpuRungeKutta.cpp:229-259): one thread evaluates
                     // pow() and broadcasts the new step size with the error norm
-                    ermax = block_max_then((double)em, red_d, [&](double emax) {
+                    ermax = group_max_then<CL>(g, (double)em, red_d, [&](double emax) {
                         const double e = __ddiv_rn(emax, P.eps);
                         double hn;
                         if (e <= 1.0)
@@ -296,10 +299,10 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
                         else
                             hn = fmax(__dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PSHRNK)),
                                       __dmul_rn(ck::HFACTOR, h));
-                        red_d[33] = hn;
+                        red_d[34] = hn;
                         return e;
                     });
-                    const double hn = red_d[33];
+                    const double hn = red_d[34];
                     if (ermax <= 1.0) { hnext = hn; break; }
                     h = hn;
                     if (__dadd_rn(t, h) == t) { underflow = true; break; }
@@ -316,18 +319,18 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
 
             // ---- CpuSat::GetClauseViolationCount on the accepted state ----
             for (int v = tid; v < n; v += nt) sy[v] = st.X[v];
-            __syncthreads();
+            g.sync();
             int cnt = 0;
             for (int m = tid; m < I.m; m += nt) cnt += clause_violated<KMAX, EXACT, ENC>(I, m, sy);
-            viol = block_sum(cnt, red_i);
+            viol = group_sum<CL>(g, cnt, red_i);
             if (viol < minviol) {
                 minviol = viol;
                 if (P.best_bits) {
                     uint32_t* bits = P.best_bits + P.unit_bits[u];
                     for (int i0 = tid & ~31; i0 < n; i0 += nt) {
                         const int i = i0 + (tid & 31);
-                        const bool b = i < n && sy[__ldg(I.iperm + (i < n ? i : 0))] > T(0);
-                        const unsigned bal = __ballot_sync(0xffffffffu, b);
+                        const bool bb = i < n && sy[__ldg(I.iperm + (i < n ? i : 0))] > T(0);
+                        const unsigned bal = __ballot_sync(0xffffffffu, bb);
                         if ((tid & 31) == 0) bits[i0 >> 5] = bal;
                     }
                 }
@@ -337,14 +340,12 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
                 if (tid == 0 && P.stop_on_first) atomicExch(P.inst_solved + pidx, 1);
                 break;
             }
+            int f = 0;
             if (tid == 0) {
-                int f = 0;
                 if (P.deadline && globaltimer_ns() >= *P.deadline) f = 1;
                 if (P.stop_on_first && atomicAdd(P.inst_solved + pidx, 0) != 0) f = 1;
-                s_flag = f;
             }
-            __syncthreads();
-            if (s_flag) { status = SAT_ODE_INTERRUPTED; break; }
+            if (g.bcast(&s_flag, f)) { status = SAT_ODE_INTERRUPTED; break; }
         }
         if (status == SAT_UNKNOWN) {
             if (t >= P.tmax) status = SAT_MAXTIME_REACHED;
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         }
 
         // write back the final state in the public layout
-        __syncthreads();
+        g.sync();
         for (int i = tid; i < n; i += nt) G[i] = st.X[__ldg(I.iperm + i)];
         for (int j = tid; j < I.m; j += nt) {
             const T v = st.X[n + __ldg(I.icperm + j)];
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
             r.pad0 = r.pad1 = 0;
             P.results[u] = r;
         }
-        __syncthreads();  // s_unit / shared buffers are reused by the next unit
+        g.sync();  // s_unit / shared buffers are reused by the next unit
     }
 }
 

@@ -63,11 +63,13 @@ def parse_args():
     ap.add_argument("--no-rhs-bench", action="store_true")
     ap.add_argument("--all-trajectories", action="store_true",
                     help="run every trajectory to its own SatResult (no early exit per instance)")
-    ap.add_argument("--workload", default="planted1000", choices=["planted1000", "uneven", "maxsat"],
+    ap.add_argument("--workload", default="planted1000",
+                    choices=["planted1000", "uneven", "maxsat", "adjoint"],
                     help="planted1000: the headline configuration; uneven: 512 planted instances "
                          "N~U{100..5000}, alpha~U(3.8,4.26), 64 trajectories each, one graph-captured "
                          "launch; maxsat: one random 4-SAT N=1e5, M=1e6 instance, 32 trajectories, "
-                         "minimise unsat over --maxsat-seconds")
+                         "minimise unsat over --maxsat-seconds; adjoint: gradients of V at T=5 for "
+                         "1024 random 3-SAT N=200, M=850 instances, FP32 vs FP64")
     ap.add_argument("--maxsat-seconds", type=float, default=60.0)
     ap.add_argument("--max-steps", type=int, default=WORKLOAD["maxsteps"],
                     help="per-trajectory step cap (profiling runs use a small one)")
@@ -516,6 +518,47 @@ def run_maxsat(args):
                       "launch_shape": s.launch_shape()}), flush=True)
 
 
+def run_adjoint(args):
+    """Gradients of V = sum w a K^2 at T=5 w.r.t. s(0), a(0) and per-clause weights for
+    1024 random 3-SAT instances (N=200, M=850), FP32 and FP64; reports gradients per
+    second, the FP32-vs-FP64 relative error, and one descent step on a(0) lowering V."""
+    import analogsat_b200 as A
+    from analogsat_b200.instances import make_instance, initial_states
+    P, n, m = 1024, 200, 850
+    raw = [make_instance("random", n, m, 3, seed=6000 + i)[:2] for i in range(P)]
+    probs = [A.SatProblem.from_arrays(l, c) for l, c in raw]
+    X = np.concatenate([initial_states(n, m, 1, seed=60_000 + i) for i in range(P)])
+    w = np.random.default_rng(6).uniform(0.5, 1.5, size=P * m)
+    out = {}
+    for prec, dt in ((A.AS_PREC_F32_LOGA, np.float32), (A.AS_PREC_F64, np.float64)):
+        s = A.SatSolver(probs, precision=prec)
+        s.SetEpsilon(1e-6)
+        s.SetSatStates(np.arange(P, dtype=np.int32), X.astype(dt))
+        s.Adjoint(5.0, weights=w)  # warm-up
+        t0 = time.perf_counter()
+        g = s.Adjoint(5.0, weights=w)
+        out[prec] = (time.perf_counter() - t0, g, s)
+    t32, g32, s32 = out[A.AS_PREC_F32_LOGA]
+    t64, g64, s64 = out[A.AS_PREC_F64]
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    # one projected descent step on a(0) (clause weights' initial values) with FP64 gradients
+    Xr = X.reshape(P, n + m)
+    ga = g64["grad_x0"].reshape(P, n + m)[:, n:]
+    step = 0.5 / np.maximum(np.abs(ga).max(axis=1, keepdims=True), 1e-30)
+    X2 = Xr.copy()
+    X2[:, n:] = np.maximum(Xr[:, n:] - step * ga, 1e-3)
+    s64.SetSatStates(np.arange(P, dtype=np.int32), X2)
+    g2 = s64.Adjoint(5.0, weights=w)
+    print(json.dumps({"workload": "adjoint-random-3sat-N200-M850-x1024-T5",
+                      "fp32_s": t32, "fp64_s": t64, "gradients_per_s_fp32": P / t32,
+                      "gradients_per_s_fp64": P / t64, "median_steps": float(np.median(g64["nsteps"])),
+                      "fp32_vs_fp64_rel_err_grad_x0": rel(g32["grad_x0"], g64["grad_x0"]),
+                      "fp32_vs_fp64_rel_err_grad_w": rel(g32["grad_w"], g64["grad_w"]),
+                      "fp32_vs_fp64_rel_err_loss": rel(g32["loss"], g64["loss"]),
+                      "mean_loss_before_a0_step": float(g64["loss"].mean()),
+                      "mean_loss_after_a0_step": float(g2["loss"].mean())}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -524,6 +567,8 @@ def main():
         run_uneven(args)
     elif args.workload == "maxsat":
         run_maxsat(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_ours(args)
 

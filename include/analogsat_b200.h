@@ -197,6 +197,10 @@ int32_t as_solver_force_threads(as_solver* s, int32_t threads);
 #define AS_STORAGE_SHARED 1
 #define AS_STORAGE_GLOBAL 2
 int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode);
+/* CTAs per trajectory in global-storage mode (no reference counterpart): 0 picks
+ * automatically (a thread-block cluster of 4 or 8 CTAs when there are few
+ * trajectories, so that they still cover the whole GPU), 1, 4 or 8 force it. */
+int32_t as_solver_set_cluster_size(as_solver* s, int32_t ctas);
 
 /* ---- gradients (no counterpart in the reference: it has no differentiation) --
  * Weighted CTDS: a_m -> w_m a_m in the potential and the spin equation

@@ -46,6 +46,30 @@ def test_global_storage_matches_shared_memory(precision):
     assert np.array_equal(out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("cl", [4, 8])
+def test_cluster_storage_matches_single_cta(cl):
+    """A trajectory spread over a thread-block cluster (cluster barriers, distributed
+    shared memory reductions) gives bit-identical results to one CTA per trajectory."""
+    from analogsat_b200 import SatProblem
+    from analogsat_b200.instances import make_instance, initial_states
+    n, m, T = 2500, 10625, 6
+    lits, lens, _ = make_instance("planted", n, m, 3, seed=21)
+    p = SatProblem.from_arrays(lits, lens)
+    ics = initial_states(n, m, T, seed=9, dtype=np.float32)
+    out = []
+    for c in (1, cl):
+        s = _solver([p], 0, batch=20, maxsteps=400)
+        s.SetStorageMode(2)
+        s.SetClusterSize(c)
+        s.SetSatStates(np.zeros(T, np.int32), ics)
+        s.Solve()
+        assert s.launch_shape()["ctas"] % c == 0
+        out.append((s.results(), s.GetSatStates(np.float32)))
+    for key in out[0][0]:
+        assert np.array_equal(out[0][0][key], out[1][0][key]), key
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_large_instance_rhs_and_counts(oracle):
     """N=6000, M=25500: beyond the compact encoding (more than 65535 slots)."""
     from analogsat_b200 import SatProblem, get_derivatives, clause_violation_counts
