@@ -244,7 +244,7 @@ __device__ __forceinline__ void load_weights(const DevInstance& I, const Adjoint
 template <typename T, int KMAX, bool EXACT>
 __global__ void __launch_bounds__(1024, 1) adj_forward_kernel(AdjointParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[35];
+    __shared__ double red_d[36];
     __shared__ int s_unit;
     const int tid = threadIdx.x, nt = blockDim.x;
     while (true) {
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(1024, 1) adj_forward_kernel(AdjointParams P) {
 template <typename T, int KMAX, bool EXACT>
 __global__ void __launch_bounds__(1024, 1) adj_backward_kernel(AdjointParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[35];
+    __shared__ double red_d[36];
     __shared__ int s_unit;
     const int tid = threadIdx.x, nt = blockDim.x;
     while (true) {

@@ -237,8 +237,8 @@ struct Grp {
 };
 
 // Group-wide max (FP64) post-processed by one thread: fn(max) is broadcast to every
-// thread.  red: 35 doubles of shared memory per CTA -- [0,32) warp partials, [32] the
-// CTA partial, [33] the result; fn may publish more values in red[34].
+// thread.  red: 36 doubles of shared memory per CTA -- [0,32) warp partials, [32] the
+// CTA partial, [33] the result; fn may publish more values in red[34] and red[35].
 template <int CL, typename F>
 __device__ __forceinline__ double group_max_then(const Grp<CL>& g, double v, double* red, F&& fn) {
 #pragma unroll

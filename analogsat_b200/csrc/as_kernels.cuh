@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
     constexpr int ENC = GS ? 1 : 0;
     using S = Solver<T, LOGA, KMAX, EXACT, ENC, CL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double red_d[35];
+    __shared__ double red_d[36];
     __shared__ int red_i[33];
     __shared__ int s_unit, s_flag;
     const Grp<CL> g;
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         if (skip) status = SAT_ODE_INTERRUPTED;
 
         while (status == SAT_UNKNOWN && t < P.tmax && steps < P.maxsteps) {
-            bool underflow = false;
+            bool underflow = false, interrupted = false;
             int taken = 0;
             for (int b = 0; b < P.batch; b++) {
                 // ---- CpuRungeKutta::Step, count = 1 ----
@@ -300,14 +300,24 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
                             hn = fmax(__dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PSHRNK)),
                                       __dmul_rn(ck::HFACTOR, h));
                         red_d[34] = hn;
+                        // early exit between batch checks: another trajectory solved this
+                        // instance, or the wall-clock budget ran out (no extra barrier).  A
+                        // cluster evaluates fn in every CTA, so it keeps to the batch-end check
+                        // (decided once and broadcast) to stay uniform.
+                        bool quit = false;
+                        if constexpr (CL == 1)
+                            quit = (P.stop_on_first && atomicAdd(P.inst_solved + pidx, 0) != 0) ||
+                                   (P.deadline && globaltimer_ns() >= *P.deadline);
+                        red_d[35] = quit ? 1.0 : 0.0;
                         return e;
                     });
                     const double hn = red_d[34];
+                    if (red_d[35] != 0.0) { interrupted = true; break; }
                     if (ermax <= 1.0) { hnext = hn; break; }
                     h = hn;
                     if (__dadd_rn(t, h) == t) { underflow = true; break; }
                 }
-                if (underflow) break;
+                if (underflow || interrupted) break;
                 hdid = h;
                 t = __dadd_rn(t, h);
                 taken++;
@@ -316,6 +326,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
             }
             if (underflow) { status = SAT_UNDERFLOW; break; }
             steps += taken;
+            if (interrupted) { status = SAT_ODE_INTERRUPTED; break; }
 
             // ---- CpuSat::GetClauseViolationCount on the accepted state ----
             for (int v = tid; v < n; v += nt) sy[v] = st.X[v];
