@@ -20,6 +20,7 @@ AS_ERR_UNSUPPORTED = -4
 AS_ERR_IO = -5
 AS_PREC_F32_LOGA = 0
 AS_PREC_F64 = 1
+AS_LAYOUT_F32_PAIR = 2  # layout_stats only
 
 _vp = C.c_void_p
 _i32 = C.c_int32

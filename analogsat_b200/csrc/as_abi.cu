@@ -20,6 +20,9 @@
 
 using namespace asb;
 
+// layout index of the pair RHS kernel's packing (after the two precisions)
+constexpr int kLayoutPair = AS_LAYOUT_F32_PAIR;
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -55,7 +58,7 @@ struct DevBuf {
 // Device copy of one or more packed instances in a single pool.
 struct DevicePool {
     int device = -1;
-    DevBuf lit, litw, slotw, srow, perm, iperm, icperm, inst;
+    DevBuf lit, litw, slotw, srow, perm, iperm, icperm, cperm, inst;
     std::vector<DevInstance> host_inst;
 
     template <typename V>
@@ -82,6 +85,7 @@ struct DevicePool {
         AS_CUDA(perm.alloc(std::max<size_t>(np, 1) * 4));
         AS_CUDA(iperm.alloc(std::max<size_t>(np, 1) * 4));
         AS_CUDA(icperm.alloc(std::max<size_t>(nc, 1) * 4));
+        AS_CUDA(cperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
         host_inst.clear();
         size_t ol = 0, ow = 0, orr = 0, op = 0, oc = 0;
@@ -96,10 +100,12 @@ struct DevicePool {
             d.perm = perm.as<int32_t>() + op;
             d.iperm = iperm.as<int32_t>() + op;
             d.icperm = icperm.as<int32_t>() + oc;
+            d.cperm = cperm.as<int32_t>() + oc;
             int r;
             if ((r = put(lit, ol, q->lit)) || (r = put(litw, ow, q->litw)) || (r = put(slotw, ow, q->slotw)) ||
                 (r = put(srow, orr, q->srow)) || (r = put(perm, op, q->perm)) ||
-                (r = put(iperm, op, q->iperm)) || (r = put(icperm, oc, q->icperm)))
+                (r = put(iperm, op, q->iperm)) || (r = put(icperm, oc, q->icperm)) ||
+                (r = put(cperm, oc, q->cperm)))
                 return r;
             ol += q->lit.size();
             ow += q->litw.size();
@@ -199,21 +205,24 @@ __global__ void stamp_deadline_kernel(unsigned long long* out, unsigned long lon
 // ---------------------------------------------------------------------------
 struct as_problem {
     HostProblem host;
-    // [AS_PREC_F32_LOGA]: literals may be reordered; [AS_PREC_F64]: reference order.
-    // Packed on first use of each precision.
-    PackedProblem packed_[2];
-    bool have_[2] = {false, false};
+    // [AS_PREC_F32_LOGA]: literals may be reordered; [AS_PREC_F64]: reference order;
+    // [kLayoutPair]: the two-states-per-element RHS kernel's grouping.
+    // Packed on first use of each layout.
+    PackedProblem packed_[3];
+    bool have_[3] = {false, false, false};
     std::mutex mu_;
-    DevicePool dev[2];        // lazily uploaded for the device primitives
-    DevBuf slab[2];           // per-CTA storage of the global-storage primitives
+    DevicePool dev[3];        // lazily uploaded for the device primitives
+    DevBuf slab[3];           // per-CTA storage of the global-storage primitives
 
-    const PackedProblem& packed(int prec) {
+    const PackedProblem& packed(int layout) {
         std::lock_guard<std::mutex> lock(mu_);
-        if (!have_[prec]) {
-            packed_[prec] = pack(host, prec == AS_PREC_F32_LOGA);
-            have_[prec] = true;
+        if (!have_[layout]) {
+            packed_[layout] = pack(host, layout == AS_PREC_F32_LOGA ? kPackF32
+                                         : layout == AS_PREC_F64    ? kPackReference
+                                                                    : kPackF32Pair);
+            have_[layout] = true;
         }
-        return packed_[prec];
+        return packed_[layout];
     }
     void pack_all() {}
 };
@@ -346,7 +355,7 @@ int32_t as_problem_get_clauses(const as_problem* p, int32_t* literals, int32_t* 
 
 int32_t as_problem_layout_stats(const as_problem* p, int32_t precision, int32_t* nslots,
                                 int32_t* max_degree, int64_t* bank_wavefronts, int32_t* compact) {
-    if (!p || (precision != AS_PREC_F32_LOGA && precision != AS_PREC_F64))
+    if (!p || (precision != AS_PREC_F32_LOGA && precision != AS_PREC_F64 && precision != AS_LAYOUT_F32_PAIR))
         return fail(AS_ERR_BAD_INPUT, "as_problem_layout_stats: bad argument");
     const auto& q = const_cast<as_problem*>(p)->packed(precision);
     if (nslots) *nslots = q.nslots;
@@ -400,10 +409,46 @@ int launch_per_state(as_problem* p, int prec, void (*fs)(DevInstance, const T*, 
     return AS_OK;
 }
 
+// Two states per CTA pass with packed FP32x2 arithmetic (FP32, compact instances whose
+// pair-kernel footprint fits one SM's shared memory); *done = false leaves the call to
+// the one-state kernel.
+template <bool LOGA, int KMAX, bool EXACT>
+int launch_rhs_pair(as_problem* p, const float* x, float* d, int ns, cudaStream_t st, bool* done) {
+    constexpr int BT = 1024;
+    *done = false;
+    if (reinterpret_cast<uintptr_t>(x) & 3u) return AS_OK;
+    const auto& q = p->packed(kLayoutPair);
+    int dev = 0, sms = 0, optin = 0, occ = 0;
+    AS_CUDA(cudaGetDevice(&dev));
+    AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t smem = rhs2_smem_bytes(q.n, q.m, q.nslots);
+    if (!q.compact || smem + 1024 > (size_t)optin) return AS_OK;
+    int r = ensure_uploaded(p, kLayoutPair);
+    if (r) return r;
+    auto fn = &rhs_pair_kernel<LOGA, KMAX, EXACT, BT>;
+    AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
+    if (occ < 1) return AS_OK;
+    const int grid = std::max(1, std::min((ns + 1) / 2, sms * occ));
+    // bulk stores need dxdt congruent with x mod 16 bytes (same staging offsets)
+    const int bulk_out = ((reinterpret_cast<uintptr_t>(x) - reinterpret_cast<uintptr_t>(d)) & 15u) == 0;
+    fn<<<grid, BT, smem, st>>>(p->dev[kLayoutPair].host_inst[0], x, d, ns, (long long)(q.n + q.m),
+                               bulk_out);
+    AS_CUDA(cudaGetLastError());
+    *done = true;
+    return AS_OK;
+}
+
 template <typename T, bool LOGA, int KMAX, bool EXACT>
 int launch_rhs(as_problem* p, const T* x, T* d, int ns, cudaStream_t st) {
     constexpr int BT = 512;
     constexpr int prec = sizeof(T) == 8 ? AS_PREC_F64 : AS_PREC_F32_LOGA;
+    if constexpr (sizeof(T) == 4 && EXACT) {
+        bool done = false;
+        const int r = launch_rhs_pair<LOGA, KMAX, EXACT>(p, x, d, ns, st, &done);
+        if (r || done) return r;
+    }
     const auto& q = p->packed(prec);
     return launch_per_state<T, T>(p, prec, &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT, false>,
                                   &rhs_batch_kernel<T, LOGA, KMAX, EXACT, BT, true>, BT,

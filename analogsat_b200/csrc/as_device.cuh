@@ -33,6 +33,7 @@ struct DevInstance {
     const int32_t* perm;    // internal -> public variable
     const int32_t* iperm;   // public -> internal variable
     const int32_t* icperm;  // public -> internal clause
+    const int32_t* cperm;   // internal -> public clause
 };
 
 constexpr float kInvLn2 = 1.4426950408889634f;  // d(log2 a)/dt = (da/dt) / (a ln 2)

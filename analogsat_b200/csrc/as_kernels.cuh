@@ -430,6 +430,261 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
     }
 }
 
+// ---------------------------------------------------------------------------
+// Standalone batched RHS, two states per CTA pass (FP32): the spins and the clause
+// contributions are held as float2 pairs, so the literal loads, index arithmetic and
+// loop control are shared by the two states and the arithmetic runs as packed FP32x2
+// (FFMA2/FMUL2/FADD2).  Products are formed in the one-state kernel's order (2 r =
+// (km knorm)(2 a) is exact scaling).
+//
+// Data movement: two consecutive public states (contiguous in HBM) arrive in a shared
+// staging buffer with one 1-D bulk copy (cp.async.bulk, mbarrier completion) that is
+// issued one pair ahead; the < 16-byte ragged ends of a row pair that does not start
+// on a 16-byte boundary are fetched with plain loads.  The kernel then works in the
+// public layout in place: a_m is read from and da_m written to its public position
+// (the pair packing makes the 32 clauses of a warp hit 32 different banks there), ds
+// is scattered to the public spin positions, and the finished pair leaves with one
+// bulk store (when dxdt and x are congruent mod 16 bytes; plain coalesced stores
+// otherwise).  Two staging buffers alternate: pair i is stored from one while pair
+// i+1 lands in the other.  A wait that does not complete within two seconds (it
+// cannot, short of a broken device) turns every output of the CTA's remaining pairs
+// into NaN instead of hanging.
+// Shared layout: 2 mbarriers | staging[2] (2 stride + 3 floats each) | sy2 | cs2.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline size_t rhs2_stage_floats(long long stride) {
+    return (size_t)((2 * stride + 3 + 3) & ~3ll);
+}
+__host__ __device__ inline size_t rhs2_smem_bytes(int n, int m, int nslots) {
+    return 16 + 8 * rhs2_stage_floats((long long)n + m) +
+           8 * ((size_t)((n + 1 + 3) & ~3) + (size_t)nslots + 1);
+}
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase `parity` of b to complete; false after `ns` nanoseconds.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* b, uint32_t parity, unsigned long long ns) {
+    if (mbar_test(b, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_test(b, parity))
+        if (globaltimer_ns() - t0 > ns) return false;
+    return true;
+}
+// 1-D bulk copy global -> shared, completion counted on b (no multicast).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(b))
+        : "memory");
+}
+
+// 1-D bulk copy shared -> global in the CTA's bulk group; the source must stay
+// unchanged until bulk_wait_read() returns.
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_addr(src)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// Row pair `pr` of x as it lands in the staging buffer: stg[off + e] = x[2 pr stride + e].
+struct PairCopy {
+    const float* src;
+    int cnt;   // floats (one or two rows)
+    int off;   // staging offset, keeps shared and global addresses congruent mod 16
+    int head;  // plain-loaded floats before the first 16-byte boundary
+    int nb;    // floats moved by the bulk copy (multiple of 4)
+    __device__ PairCopy(const float* x, int pr, int ntraj, long long stride) {
+        src = x + (long long)(2 * pr) * stride;
+        cnt = (int)((2 * pr + 1 < ntraj ? 2 : 1) * stride);
+        const uint32_t mis = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 15u);
+        off = (int)(mis >> 2);
+        head = min(cnt, (int)(((16u - mis) & 15u) >> 2));
+        nb = ((cnt - head) >> 2) << 2;
+    }
+    // thread t < 6 owns one ragged float: t < 3 in the head, 3..5 in the tail
+    __device__ int ragged(int t) const {
+        const int e = t < 3 ? t : head + nb + (t - 3);
+        return (t < 3 ? e < head : e < cnt) ? e : -1;
+    }
+};
+
+template <bool LOGA, int KMAX, bool EXACT, int BT>
+__global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const float* __restrict__ x,
+                                                          float* __restrict__ dxdt, int ntraj,
+                                                          long long stride, int bulk_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
+    const size_t sf = rhs2_stage_floats(stride);
+    float* stg0 = reinterpret_cast<float*>(smem_raw + 16);
+    float2* sy = reinterpret_cast<float2*>(stg0 + 2 * sf);
+    float2* cs = sy + ((I.n + 1 + 3) & ~3);
+    const int tid = threadIdx.x;
+    const int n = I.n;
+    const float knorm = (float)ldexp(1.0, -I.k);
+    const float2 kn2 = f2(knorm);
+    const int npairs = (ntraj + 1) / 2;
+    const int G = gridDim.x;
+    constexpr unsigned long long kWaitNs = 2000000000ull;
+    int pr = blockIdx.x;
+    if (pr >= npairs) return;
+    for (int j = tid; j <= I.nslots; j += BT) cs[j] = f2(0.0f);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+    }
+    __syncthreads();
+    // Copy of pair q into buffer b: thread 0 starts the bulk part; threads 0..5 load
+    // the ragged floats into rag (stored into the buffer at the top of the iteration
+    // that consumes it).
+    float rag = 0.0f;
+    int rag_at = -1;  // float index into stg0 (buffer offset included), or -1
+    auto issue = [&](int q, int b) {
+        const PairCopy c(x, q, ntraj, stride);
+        float* dst = stg0 + (size_t)b * sf;
+        if (tid == 0) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive_tx(bar + b, (uint32_t)c.nb * 4u);
+            if (c.nb > 0) bulk_load(dst + c.off + c.head, c.src + c.head, (uint32_t)c.nb * 4u, bar + b);
+        }
+        if (tid < 6) {
+            const int e = c.ragged(tid);
+            rag_at = e >= 0 ? b * (int)sf + c.off + e : -1;
+            if (e >= 0) rag = __ldg(c.src + e);
+        }
+    };
+    issue(pr, 0);
+    uint32_t parity = 0;  // bit b: phase parity expected next on bar[b]
+    for (int it = 0; pr < npairs; pr += G, it++) {
+        const int b = it & 1;
+        if (rag_at >= 0) stg0[rag_at] = rag;
+        rag_at = -1;
+        const bool ok = mbar_wait_for(bar + b, (parity >> b) & 1u, kWaitNs);
+        if (__syncthreads_or(!ok)) {
+            mbar_wait_for(bar + b, (parity >> b) & 1u, kWaitNs);  // let a late copy land
+            if (tid == 0) bulk_wait_all();
+            const float nan = __int_as_float(0x7fc00000);
+            for (; pr < npairs; pr += G) {
+                const long long cnt = (2 * pr + 1 < ntraj ? 2 : 1) * stride;
+                for (long long e = tid; e < cnt; e += BT) dxdt[(long long)(2 * pr) * stride + e] = nan;
+            }
+            return;
+        }
+        parity ^= 1u << b;
+        const bool two = 2 * pr + 1 < ntraj;
+        const PairCopy cur(x, pr, ntraj, stride);
+        float* S0 = stg0 + (size_t)b * sf + cur.off;
+        float* S1 = two ? S0 + stride : S0;
+        // spins into internal order, interleaved
+#pragma unroll 2
+        for (int v = tid; v < n; v += BT) {
+            const int p = __ldg(I.perm + v);
+            sy[v] = make_float2(S0[p], S1[p]);
+        }
+        if (tid == 0) sy[n] = f2(-1.0f);
+        __syncthreads();
+        if (pr + G < npairs) {
+            // the other buffer held pair pr - G: its bulk store must have read it out
+            if (tid == 0 && bulk_out) bulk_wait_read();
+            issue(pr + G, b ^ 1);
+        }
+        // clause phase: a_m in, da_m out at the public clause position
+        for (int m = tid; m < I.m; m += BT) {
+            Lit<0> w[KMAX];
+            float2 f[KMAX];
+            float2 km = kn2;
+            const int j = n + ld_ro(I.cperm + m);
+#pragma unroll
+            for (int q = 0; q < KMAX; q++) {
+                if (EXACT || q < I.k) {
+                    w[q].load(I, q * I.mp + m);
+                    const float c = w[q].neg() ? 1.0f : -1.0f;  // f = 1 - c_lit s = 1 + c s
+                    f[q] = __ffma2_rn(f2(c), sy[w[q].var()], f2(1.0f));
+                    km = __fmul2_rn(km, f[q]);
+                }
+            }
+            const float2 a = make_float2(S0[j], S1[j]);
+            float2 am;
+            if constexpr (LOGA) am = make_float2(exp2_fast(a.x), exp2_fast(a.y));
+            else am = a;
+            // da: (km km) / ln 2 in log space, (a km) km otherwise, as in the one-state kernel
+            const float2 da = LOGA ? __fmul2_rn(__fmul2_rn(km, km), f2(kInvLn2))
+                                   : __fmul2_rn(__fmul2_rn(am, km), km);
+            S0[j] = da.x;
+            S1[j] = da.y;
+            const float2 r2 = __fmul2_rn(__fmul2_rn(km, kn2), __fmul2_rn(am, f2(2.0f)));
+#pragma unroll
+            for (int q = 0; q < KMAX; q++) {
+                if (EXACT || q < I.k) {
+                    float2 prod = f2(1.0f);
+                    bool first = true;
+#pragma unroll
+                    for (int l = 0; l < KMAX; l++) {
+                        if (l != q && (EXACT || l < I.k)) {
+                            prod = first ? f[l] : __fmul2_rn(prod, f[l]);
+                            first = false;
+                        }
+                    }
+                    cs[w[q].slot()] = __fmul2_rn(__fmul2_rn(r2, prod), f2(w[q].neg() ? -1.0f : 1.0f));
+                }
+            }
+        }
+        __syncthreads();
+        // var phase: ds_i to the public spin position
+        for (int v = tid; v < n; v += BT) {
+            const int g = v >> 5;
+            const int r0 = ld_ro(I.srow + g), r1 = ld_ro(I.srow + g + 1);
+            const float2* p = cs + r0 * 32 + (v & 31);
+            float2 sum = f2(0.0f);
+#pragma unroll 4
+            for (int r = r0; r < r1; r++, p += 32) sum = __fadd2_rn(sum, *p);
+            const int pv = __ldg(I.perm + v);
+            S0[pv] = sum.x;
+            S1[pv] = sum.y;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // results -> bulk store
+        __syncthreads();
+        float* D = dxdt + (long long)(2 * pr) * stride;
+        if (bulk_out) {
+            if (tid == 0 && cur.nb > 0) bulk_store(D + cur.head, S0 + cur.head, (uint32_t)cur.nb * 4u);
+            if (tid < 6) {
+                const int e = cur.ragged(tid);
+                if (e >= 0) D[e] = S0[e];
+            }
+        } else {
+            for (int e = tid; e < cur.cnt; e += BT) D[e] = S0[e];
+        }
+        // no barrier here: the next writes to this buffer, sy and cs all come after
+        // the next iteration's barriers
+    }
+    if (tid == 0) bulk_wait_all();
+}
+
 // Exact unsat counts of many states: one CTA per state.
 template <typename T, int KMAX, bool EXACT, int BT, bool GS>
 __global__ void __launch_bounds__(BT) viol_batch_kernel(DevInstance I, const T* __restrict__ x,

@@ -96,14 +96,17 @@ namespace {
 // banks (optionally after reordering its literals) are all still free in their
 // slots; when no candidate within a search window fits, complete the group with the
 // least-conflicting candidates.  Deterministic (fixed seed).
-void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
+void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute, bool pairs,
                       std::vector<std::vector<int8_t>>& order) {
     const int m = p.m, k = p.k;
     order.assign(m, {});
     q.cperm.resize(m);
     q.icperm.resize(m);
+    // 32-bit layouts: bank = internal variable mod 32, one set of 32 lanes;
+    // pair layout: bank pair = internal variable mod 16, per 16-lane half
+    const int lanes = pairs ? 16 : 32;
     std::vector<int32_t> bank(p.storage.size());
-    for (size_t i = 0; i < p.storage.size(); i++) bank[i] = q.iperm[std::abs(p.storage[i]) - 1] & 31;
+    for (size_t i = 0; i < p.storage.size(); i++) bank[i] = q.iperm[std::abs(p.storage[i]) - 1] & (lanes - 1);
     // candidate literal orders per clause length (all permutations for k <= 4)
     auto perms_for = [&](int len) {
         std::vector<std::vector<int8_t>> ps;
@@ -124,18 +127,23 @@ void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
         std::swap(rem[j], rem[rng % (uint64_t)(j + 1)]);
     }
     const int kw = std::min(k, 16);
+    // candidates tried per lane (first fit), and per lane of the least-conflict completion
+    const size_t kScanWindow = pairs ? 4096 : 1024;
+    const int kFillWindow = pairs ? 1024 : 256;
     int out = 0;
     long waves = 0;
     std::vector<uint32_t> used(kw);
+    uint32_t used_clause = 0;  // pair layout: public clause index mod 32 across the warp
     std::vector<int32_t> keep;
     keep.reserve(m);
     while (!rem.empty()) {
         std::fill(used.begin(), used.end(), 0u);
+        used_clause = 0;
         int filled = 0;
         keep.clear();
         size_t scanned = 0;
         auto cost = [&](int j, const std::vector<int8_t>& ord) {
-            int c = 0;
+            int c = pairs ? (int)((used_clause >> (j & 31)) & 1u) : 0;
             for (int qq = 0; qq < (int)ord.size() && qq < kw; qq++)
                 c += (used[qq] >> bank[p.start[j] + ord[qq]]) & 1u;
             return c;
@@ -143,16 +151,18 @@ void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
         auto take = [&](int j, const std::vector<int8_t>& ord) {
             for (int qq = 0; qq < (int)ord.size() && qq < kw; qq++)
                 used[qq] |= 1u << bank[p.start[j] + ord[qq]];
+            used_clause |= 1u << (j & 31);
             order[out] = ord;
             q.cperm[out] = j;
             out++;
             filled++;
+            if (filled == lanes && lanes < 32) std::fill(used.begin(), used.end(), 0u);  // second half
         };
         size_t i = 0;
         for (; i < rem.size() && filled < 32; i++) {
             const int j = rem[i];
             bool placed = false;
-            if (scanned < 1024) {
+            if (scanned < kScanWindow) {
                 scanned++;
                 for (const auto& ord : perms[p.length[j]])
                     if (cost(j, ord) == 0) { take(j, ord); placed = true; break; }
@@ -163,7 +173,7 @@ void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
         while (filled < 32 && !keep.empty()) {
             int best = 0, bc = 1 << 30;
             const std::vector<int8_t>* bo = nullptr;
-            for (int c = 0; c < (int)keep.size() && c < 256; c++) {
+            for (int c = 0; c < (int)keep.size() && c < kFillWindow; c++) {
                 for (const auto& ord : perms[p.length[keep[c]]]) {
                     const int cc = cost(keep[c], ord);
                     if (cc < bc) { bc = cc; best = c; bo = &ord; }
@@ -179,11 +189,11 @@ void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
         rem.swap(keep);
     }
     for (int mi = 0; mi < m; mi++) q.icperm[q.cperm[mi]] = mi;
-    // wavefront count of one gather pass, for diagnostics
-    for (int g = 0; g < m; g += 32) {
+    // wavefront count of one gather pass (per bank group of `lanes` clauses), for diagnostics
+    for (int g = 0; g < m; g += lanes) {
         for (int qq = 0; qq < kw; qq++) {
             int cnt[32] = {0}, mx = 0;
-            for (int mi = g; mi < std::min(m, g + 32); mi++) {
+            for (int mi = g; mi < std::min(m, g + lanes); mi++) {
                 const int j = q.cperm[mi];
                 if (qq < p.length[j]) mx = std::max(mx, ++cnt[bank[p.start[j] + order[mi][qq]]]);
             }
@@ -195,7 +205,8 @@ void schedule_clauses(const HostProblem& p, PackedProblem& q, bool permute,
 
 }  // namespace
 
-PackedProblem pack(const HostProblem& p, bool permute_literals) {
+PackedProblem pack(const HostProblem& p, int mode) {
+    const bool permute_literals = mode != kPackReference;
     PackedProblem q;
     q.n = p.n;
     q.m = p.m;
@@ -242,7 +253,7 @@ PackedProblem pack(const HostProblem& p, bool permute_literals) {
     // literal order inside each internal clause (indices into the public clause)
     std::vector<std::vector<int8_t>> order;
     if (q.compact) {
-        schedule_clauses(p, q, permute_literals, order);
+        schedule_clauses(p, q, permute_literals, mode == kPackF32Pair, order);
     } else {  // the streamed kernels read no shared-memory banks this way: keep the order
         q.cperm.resize(p.m);
         q.icperm.resize(p.m);

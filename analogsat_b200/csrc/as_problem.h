@@ -36,6 +36,12 @@
 //    clause may also be reordered for this (FP32 packing only: FP64 keeps the
 //    reference's product order to stay bit-identical).  The contribution slots
 //    keep the public (clause, literal) order either way.
+//  * Pair layout (kPackF32Pair): for the kernel that holds two states per shared
+//    array element (float2).  A 64-bit shared access is served per half-warp, and a
+//    float2 at index v sits in bank pair v mod 16, so the grouping asks instead that
+//    each 16-lane half of a warp touches 16 different bank pairs in every literal
+//    slot, and that the 32 clauses of a warp have 32 different public indices mod 32
+//    (that kernel reads and writes a_m in place in the public layout).
 #pragma once
 
 #include <cstdint>
@@ -77,6 +83,11 @@ struct PackedProblem {
     long bank_wavefronts = 0;      // shared-memory wavefronts of one gather pass (>= 32-clause groups x k)
 };
 
-PackedProblem pack(const HostProblem& p, bool permute_literals);
+enum PackMode : int {
+    kPackReference = 0,  // reference literal order (FP64, bit-identical products)
+    kPackF32 = 1,        // literals may be reordered; 32-lane bank groups
+    kPackF32Pair = 2,    // literals may be reordered; 16-lane bank-pair groups + clause banks
+};
+PackedProblem pack(const HostProblem& p, int mode);
 
 }  // namespace asb

@@ -414,7 +414,8 @@ def rhs_kernel_bench(A, problem, ics_dev, nm, st, reps=10):
     bytes_per_launch = B * 8 * nm + 4 * W["k"] * W["m"]
     # traffic: ncu dram__bytes_read + dram__bytes_write of one launch of this exact
     # configuration (profiles/rhs_batch_kernel_16384_states_N1000_M4250.md)
-    return {"bound": "hbm", "kernel": "rhs_batch_kernel", "states_per_launch": B,
+    kernel = "rhs_pair_kernel" if x.dtype == torch.float32 else "rhs_batch_kernel"
+    return {"bound": "hbm", "kernel": kernel, "states_per_launch": B,
             "ms_per_launch": ms, "achieved": bytes_per_launch / (ms / 1e3) / 1e9, "unit": "GB/s",
             "bytes_per_launch": bytes_per_launch,
             "traffic": 641.86e6 if B == 16384 else None}

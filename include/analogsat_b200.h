@@ -88,7 +88,11 @@ int32_t as_problem_get_clauses(const as_problem* p, int32_t* literals, int32_t* 
 /* Device-layout diagnostics of the packing for `precision` (no reference
  * counterpart): contribution slots, largest variable degree, shared-memory
  * wavefronts of one spin-gather pass after bank-aware clause grouping (the ideal is
- * k * ceil(M/32)), and whether the shared-memory kernels accept the instance. */
+ * k * ceil(M/32)), and whether the shared-memory kernels accept the instance.
+ * `precision` may also be AS_LAYOUT_F32_PAIR, the packing of the FP32 device RHS
+ * (as_rhs_f32) that holds two states per shared element; its wavefronts are
+ * counted per 16-lane half-warp (ideal k * ceil(M/16)). */
+#define AS_LAYOUT_F32_PAIR 2
 int32_t as_problem_layout_stats(const as_problem* p, int32_t precision, int32_t* nslots,
                                 int32_t* max_degree, int64_t* bank_wavefronts, int32_t* compact);
 

@@ -136,5 +136,9 @@ def test_packing_layout_quality():
     assert m * k <= s32["nslots"] <= 1.1 * m * k
     assert s32["bank_wavefronts"] <= 1.6 * ideal   # literal reordering allowed (FP32)
     assert s64["bank_wavefronts"] <= 2.2 * ideal   # clause regrouping only (FP64)
+    from analogsat_b200._abi import AS_LAYOUT_F32_PAIR
+    sp = p.layout_stats(AS_LAYOUT_F32_PAIR)      # 16-lane groups + public-clause banks
+    assert sp["nslots"] == s32["nslots"]
+    assert sp["bank_wavefronts"] <= 1.4 * k * ((m + 15) // 16)
     big = SatProblem.from_arrays(*make_instance("fast", 40000, 200000, 4, seed=1)[:2])
     assert not big.layout_stats()["compact"]

@@ -95,6 +95,38 @@ def test_rhs_and_counts_many_states_vs_oracle(oracle, golden):
     assert C[2] == 0  # the planted assignment satisfies every clause
 
 
+@pytest.mark.parametrize("tag", ["p1000", "r4"])
+@pytest.mark.parametrize("logspace", [False, True])
+@pytest.mark.parametrize("count,shift,oshift", [(2, 0, 0), (7, 0, 0), (64, 0, 0), (7, 1, 1), (5, 3, 3),
+                                                (6, 0, 1), (3, 2, 0)])
+def test_rhs_f32_pair_kernel_bit_identical(golden, tag, logspace, count, shift, oshift):
+    """FP32 states go through the two-states-per-pass kernel (packed FP32x2, bulk-copied
+    row pairs, results in place): each state's derivative is bit-identical whether it
+    shares a pass with another state or runs alone (odd counts; state arrays starting
+    4, 8 or 12 bytes past a 16-byte boundary; outputs congruent with the inputs mod 16
+    bytes, written by bulk stores, or not, written by plain stores)."""
+    from analogsat_b200 import get_derivatives
+    p = _prob(golden, tag)
+    nm = p.n + p.m
+    rng = np.random.default_rng(count)
+    a = rng.uniform(-1, 2, (count, p.m)) if logspace else rng.uniform(0.5, 3, (count, p.m))
+    X = np.concatenate([rng.uniform(-1, 1, (count, p.n)), a], axis=1).astype(np.float32)
+    X[0, : p.n] = np.sign(X[0, : p.n])
+    flat = torch.zeros(count * nm + 4, dtype=torch.float32, device="cuda")
+    xd = flat[shift:shift + count * nm].view(count, nm)
+    xd.copy_(torch.from_numpy(X))
+    oflat = torch.full((count * nm + 8,), 7.0, dtype=torch.float32, device="cuda")
+    out = oflat[oshift:oshift + count * nm].view(count, nm)
+    get_derivatives(p, xd, out=out, logspace=logspace)
+    D = out.cpu().numpy()
+    o = oflat.cpu().numpy()
+    assert np.all(o[:oshift] == 7.0) and np.all(o[oshift + count * nm:] == 7.0)  # nothing outside
+    assert np.array_equal(xd.cpu().numpy(), X)  # input untouched
+    for i in range(count):
+        d1 = get_derivatives(p, _cuda(X[i:i + 1], torch.float32), logspace=logspace).cpu().numpy()
+        assert np.array_equal(D[i], d1[0]), (i, np.abs(D[i] - d1[0]).max())
+
+
 def _solver(golden, tag, precision, eps, batch, maxsteps, tmax=1e8):
     from analogsat_b200 import SatSolver
     s = SatSolver([_prob(golden, tag)], precision=precision)
