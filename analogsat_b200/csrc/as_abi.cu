@@ -423,10 +423,11 @@ int launch_rhs_pair(as_problem* p, const float* x, float* d, int ns, cudaStream_
     AS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t smem = rhs2_smem_bytes(q.n, q.m, q.nslots);
-    if (!q.compact || smem + 1024 > (size_t)optin) return AS_OK;
+    constexpr int CPT = 5, VPT = 1;  // instances whose footprint fits have M <= 5 * 1024
+    if (!q.compact || smem + 1024 > (size_t)optin || q.m > CPT * BT || q.n > VPT * BT) return AS_OK;
     int r = ensure_uploaded(p, kLayoutPair);
     if (r) return r;
-    auto fn = &rhs_pair_kernel<LOGA, KMAX, EXACT, BT>;
+    auto fn = &rhs_pair_kernel<LOGA, KMAX, EXACT, BT, CPT, VPT>;
     AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
     if (occ < 1) return AS_OK;

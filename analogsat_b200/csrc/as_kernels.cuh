@@ -534,7 +534,10 @@ struct PairCopy {
     }
 };
 
-template <bool LOGA, int KMAX, bool EXACT, int BT>
+// CPT / VPT: clauses / variables per thread (M <= CPT * BT, N <= VPT * BT); a thread's
+// literal words, public clause and variable indices and SELL rows are the same for
+// every pair, so they are loaded once into registers.
+template <bool LOGA, int KMAX, bool EXACT, int BT, int CPT, int VPT>
 __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const float* __restrict__ x,
                                                           float* __restrict__ dxdt, int ntraj,
                                                           long long stride, int bulk_out) {
@@ -557,6 +560,25 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
     if (tid == 0) {
         mbar_init(bar, 1);
         mbar_init(bar + 1, 1);
+    }
+    Lit<0> lw[CPT][KMAX];
+    int lj[CPT];
+#pragma unroll
+    for (int i = 0; i < CPT; i++) {
+        const int m = tid + i * BT;
+        lj[i] = m < I.m ? n + ld_ro(I.cperm + m) : 0;
+#pragma unroll
+        for (int q = 0; q < KMAX; q++)
+            if (m < I.m && (EXACT || q < I.k)) lw[i][q].load(I, q * I.mp + m);
+            else lw[i][q].w = 0;
+    }
+    int vp[VPT];
+    uint32_t vrows[VPT];  // first row | end row << 16 (rows < 2048 for compact instances)
+#pragma unroll
+    for (int i = 0; i < VPT; i++) {
+        const int v = tid + i * BT;
+        vp[i] = v < n ? __ldg(I.perm + v) : 0;
+        vrows[i] = v < n ? (uint32_t)ld_ro(I.srow + (v >> 5)) | ((uint32_t)ld_ro(I.srow + (v >> 5) + 1) << 16) : 0u;
     }
     __syncthreads();
     // Copy of pair q into buffer b: thread 0 starts the bulk part; threads 0..5 load
@@ -601,11 +623,9 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
         float* S0 = stg0 + (size_t)b * sf + cur.off;
         float* S1 = two ? S0 + stride : S0;
         // spins into internal order, interleaved
-#pragma unroll 2
-        for (int v = tid; v < n; v += BT) {
-            const int p = __ldg(I.perm + v);
-            sy[v] = make_float2(S0[p], S1[p]);
-        }
+#pragma unroll
+        for (int i = 0; i < VPT; i++)
+            if (tid + i * BT < n) sy[tid + i * BT] = make_float2(S0[vp[i]], S1[vp[i]]);
         if (tid == 0) sy[n] = f2(-1.0f);
         __syncthreads();
         if (pr + G < npairs) {
@@ -614,15 +634,16 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
             issue(pr + G, b ^ 1);
         }
         // clause phase: a_m in, da_m out at the public clause position
-        for (int m = tid; m < I.m; m += BT) {
-            Lit<0> w[KMAX];
+#pragma unroll
+        for (int i = 0; i < CPT; i++) {
+            if (tid + i * BT >= I.m) break;
+            const Lit<0>* w = lw[i];
             float2 f[KMAX];
             float2 km = kn2;
-            const int j = n + ld_ro(I.cperm + m);
+            const int j = lj[i];
 #pragma unroll
             for (int q = 0; q < KMAX; q++) {
                 if (EXACT || q < I.k) {
-                    w[q].load(I, q * I.mp + m);
                     const float c = w[q].neg() ? 1.0f : -1.0f;  // f = 1 - c_lit s = 1 + c s
                     f[q] = __ffma2_rn(f2(c), sy[w[q].var()], f2(1.0f));
                     km = __fmul2_rn(km, f[q]);
@@ -656,16 +677,17 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
         }
         __syncthreads();
         // var phase: ds_i to the public spin position
-        for (int v = tid; v < n; v += BT) {
-            const int g = v >> 5;
-            const int r0 = ld_ro(I.srow + g), r1 = ld_ro(I.srow + g + 1);
+#pragma unroll
+        for (int i = 0; i < VPT; i++) {
+            const int v = tid + i * BT;
+            if (v >= n) break;
+            const int r0 = (int)(vrows[i] & 0xffffu), r1 = (int)(vrows[i] >> 16);
             const float2* p = cs + r0 * 32 + (v & 31);
             float2 sum = f2(0.0f);
 #pragma unroll 4
             for (int r = r0; r < r1; r++, p += 32) sum = __fadd2_rn(sum, *p);
-            const int pv = __ldg(I.perm + v);
-            S0[pv] = sum.x;
-            S1[pv] = sum.y;
+            S0[vp[i]] = sum.x;
+            S1[vp[i]] = sum.y;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // results -> bulk store
         __syncthreads();
