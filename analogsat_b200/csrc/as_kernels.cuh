@@ -644,7 +644,9 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
 #pragma unroll
             for (int q = 0; q < KMAX; q++) {
                 if (EXACT || q < I.k) {
-                    const float c = w[q].neg() ? 1.0f : -1.0f;  // f = 1 - c_lit s = 1 + c s
+                    // c = -c_lit = +1 for a negated literal, -1 otherwise (from the sign bit):
+                    // f = 1 - c_lit s = 1 + c s
+                    const float c = __int_as_float((w[q].w & 0x80000000u) ^ 0xBF800000u);
                     f[q] = __ffma2_rn(f2(c), sy[w[q].var()], f2(1.0f));
                     km = __fmul2_rn(km, f[q]);
                 }
@@ -658,7 +660,8 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
                                    : __fmul2_rn(__fmul2_rn(am, km), km);
             S0[j] = da.x;
             S1[j] = da.y;
-            const float2 r2 = __fmul2_rn(__fmul2_rn(km, kn2), __fmul2_rn(am, f2(2.0f)));
+            // -2 r (exact scaling): the contribution c_lit 2 r K_mi is then (-2 r K_mi) c
+            const float2 r2n = __fmul2_rn(__fmul2_rn(km, kn2), __fmul2_rn(am, f2(-2.0f)));
 #pragma unroll
             for (int q = 0; q < KMAX; q++) {
                 if (EXACT || q < I.k) {
@@ -671,7 +674,8 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
                             first = false;
                         }
                     }
-                    cs[w[q].slot()] = __fmul2_rn(__fmul2_rn(r2, prod), f2(w[q].neg() ? -1.0f : 1.0f));
+                    const float c = __int_as_float((w[q].w & 0x80000000u) ^ 0xBF800000u);
+                    cs[w[q].slot()] = __fmul2_rn(__fmul2_rn(r2n, prod), f2(c));
                 }
             }
         }

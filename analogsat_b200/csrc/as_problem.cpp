@@ -291,6 +291,7 @@ void repair_groups(const HostProblem& p, const std::vector<int32_t>& bank, int l
     const int G = (int)groups.size();
     if (G < 2) return;
     std::vector<int32_t> cnt((size_t)G * 32, 0), cj((size_t)G * 32, 0);
+    const int kClauseClash = 3;  // as in schedule_balanced
     auto warp = [&](int g) { return pairs ? g / 2 : g; };
     for (int g = 0; g < G; g++)
         for (int j : groups[g]) {
@@ -330,8 +331,8 @@ void repair_groups(const HostProblem& p, const std::vector<int32_t>& bank, int l
             const int rc = c & 31, rd = d & 31;
             const size_t wa = (size_t)warp(a) * 32, wb = (size_t)warp(b) * 32;
             auto ex = [](int v) { return std::max(0, v - 1); };
-            e += ex(cj[wa + rc] - 1) - ex(cj[wa + rc]) + ex(cj[wa + rd] + 1) - ex(cj[wa + rd]);
-            e += ex(cj[wb + rd] - 1) - ex(cj[wb + rd]) + ex(cj[wb + rc] + 1) - ex(cj[wb + rc]);
+            e += kClauseClash * (ex(cj[wa + rc] - 1) - ex(cj[wa + rc]) + ex(cj[wa + rd] + 1) - ex(cj[wa + rd]));
+            e += kClauseClash * (ex(cj[wb + rd] - 1) - ex(cj[wb + rd]) + ex(cj[wb + rc] + 1) - ex(cj[wb + rc]));
         }
         return e;
     };
@@ -374,6 +375,58 @@ void repair_groups(const HostProblem& p, const std::vector<int32_t>& bank, int l
             }
         }
         if (!changed) break;
+    }
+}
+
+// Pair layout: make the public clause indices of every warp distinct mod 32 by swapping
+// a repeated clause with a clause of another warp that has the same sorted bank tuple
+// (so every group keeps its bank counts) and whose index is free here, while the
+// repeated one's index is free there.
+void fix_clause_banks(const HostProblem& p, const std::vector<int32_t>& bank, int k,
+                      std::vector<std::vector<int32_t>>& groups) {
+    const int G = (int)groups.size();
+    auto key_of = [&](int j) {
+        int b[16];
+        const int len = std::min(p.length[j], 16);
+        for (int i = 0; i < len; i++) b[i] = bank[p.start[j] + i];
+        std::sort(b, b + len);
+        uint64_t key = (uint64_t)len;
+        for (int i = 0; i < len; i++) key = key * 33 + (uint64_t)b[i];
+        return key;
+    };
+    std::unordered_map<uint64_t, std::vector<int32_t>> by_key;
+    std::vector<std::pair<int, int>> where(p.m);
+    std::vector<int32_t> cj((size_t)(G / 2 + 1) * 32, 0);
+    for (int g = 0; g < G; g++)
+        for (int u = 0; u < (int)groups[g].size(); u++) {
+            const int j = groups[g][u];
+            where[j] = {g, u};
+            by_key[key_of(j)].push_back(j);
+            cj[(size_t)(g / 2) * 32 + (j & 31)]++;
+        }
+    (void)k;
+    for (int w = 0; 2 * w < G; w++) {
+        for (int g = 2 * w; g < std::min(G, 2 * w + 2); g++) {
+            for (int u = 0; u < (int)groups[g].size(); u++) {
+                const int c = groups[g][u];
+                if (cj[(size_t)w * 32 + (c & 31)] <= 1) continue;
+                for (int d : by_key[key_of(c)]) {
+                    const int h = where[d].first, wb = h / 2;
+                    if (wb == w || cj[(size_t)w * 32 + (d & 31)] != 0) continue;
+                    if (cj[(size_t)wb * 32 + (c & 31)] - ((d & 31) == (c & 31)) != 0) continue;
+                    const int v = where[d].second;
+                    cj[(size_t)w * 32 + (c & 31)]--;
+                    cj[(size_t)w * 32 + (d & 31)]++;
+                    cj[(size_t)wb * 32 + (d & 31)]--;
+                    cj[(size_t)wb * 32 + (c & 31)]++;
+                    groups[g][u] = d;
+                    groups[h][v] = c;
+                    where[d] = {g, u};
+                    where[c] = {h, v};
+                    break;
+                }
+            }
+        }
     }
 }
 
@@ -423,10 +476,13 @@ void schedule_balanced(const HostProblem& p, PackedProblem& q, bool pairs,
     const size_t kScanWindow = 4096;
     const int kFillWindow = 1024;
     const int kEnd = 3;  // lanes left to the exact cover
+    // a repeated clause bank costs four extra wavefronts (two loads, two stores of a_m)
+    // against two for a literal bank (one gather, one store): weigh it accordingly
+    const int kClauseClash = 3;
     int cnt[32];
     uint32_t used_clause = 0;
     auto over = [&](int j) {  // literals beyond k per bank if j joins, + clause-bank clash
-        int add[32] = {0}, o = pairs ? (int)((used_clause >> (j & 31)) & 1u) : 0;
+        int add[32] = {0}, o = pairs ? kClauseClash * (int)((used_clause >> (j & 31)) & 1u) : 0;
         for (int i = 0; i < p.length[j]; i++) {
             const int b = bank[p.start[j] + i];
             if (cnt[b] + ++add[b] > k) o++;
@@ -524,6 +580,7 @@ void schedule_balanced(const HostProblem& p, PackedProblem& q, bool pairs,
         }
     }
     repair_groups(p, bank, lanes, k, pairs, groups);
+    if (pairs) fix_clause_banks(p, bank, k, groups);
     out = 0;
     for (const auto& g : groups) {
         gb.assign(g.size(), {});
