@@ -360,8 +360,8 @@ def run_ours(args):
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      # ncu dram__bytes_read+write of one solve_kernel launch over 148
                      # trajectories (profiles/solve_kernel_planted3sat_N1000_M4250.md):
-                     # 3.31 MB, i.e. 22.4 KB per trajectory, scaled to this launch
-                     "traffic": 3.31e6 / 148 * len(pidx),
+                     # 3.30 MB, i.e. 22.3 KB per trajectory, scaled to this launch
+                     "traffic": 3.298e6 / 148 * len(pidx),
                      "note": "achieved = RHS evals x 8(N+M)+4KM bytes / kernel time; state, "
                              "stages and contributions stay on chip (shared memory), so DRAM "
                              "traffic is far below the algorithmic bytes"},
@@ -413,12 +413,12 @@ def rhs_kernel_bench(A, problem, ics_dev, nm, st, reps=10):
     # per launch (T_share = all B states of the launch)
     bytes_per_launch = B * 8 * nm + 4 * W["k"] * W["m"]
     # traffic: ncu dram__bytes_read + dram__bytes_write of one launch of this exact
-    # configuration (profiles/rhs_batch_kernel_16384_states_N1000_M4250.md)
+    # configuration (profiles/rhs_pair_kernel_16384_states_N1000_M4250.md)
     kernel = "rhs_pair_kernel" if x.dtype == torch.float32 else "rhs_batch_kernel"
     return {"bound": "hbm", "kernel": kernel, "states_per_launch": B,
             "ms_per_launch": ms, "achieved": bytes_per_launch / (ms / 1e3) / 1e9, "unit": "GB/s",
             "bytes_per_launch": bytes_per_launch,
-            "traffic": 641.86e6 if B == 16384 else None}
+            "traffic": 640.34e6 if B == 16384 else None}
 
 
 def solver_groups(solver):
