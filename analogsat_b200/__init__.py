@@ -242,7 +242,8 @@ class SatSolver:
         check(self._lib.as_solver_set_cluster_size(self._h, int(ctas)))
 
     def SetStorageMode(self, mode: int):
-        """0 automatic, 1 shared memory only, 2 global storage (per-CTA slab) only."""
+        """0 automatic, 1 shared memory only, 2 global storage (per-CTA slab) only,
+        3 streamed (four trajectories per lane group, per-stage kernels over the GPU)."""
         check(self._lib.as_solver_set_storage_mode(self._h, int(mode)))
 
     # -- states (SatSolver::SetSatState, SatSolver.h:183-192) --

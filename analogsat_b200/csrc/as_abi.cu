@@ -17,6 +17,7 @@
 #include "../../include/analogsat_b200.h"
 #include "as_kernels.cuh"
 #include "as_problem.h"
+#include "as_stream.cuh"
 
 using namespace asb;
 
@@ -227,6 +228,18 @@ struct as_problem {
     void pack_all() {}
 };
 
+// Device storage and the per-pass graph of the streamed solver (AS_STORAGE_STREAM).
+struct StreamPlan {
+    int ngroups = 0;
+    std::vector<int> gprob;     // problem of each group
+    std::vector<size_t> goff;   // byte offset of each group's vectors in vec
+    std::vector<size_t> gcand;  // word offset of each group's candidate assignments
+    DevBuf vec, lanes, tickets, active, cand;
+    cudaGraphExec_t graph = nullptr;
+    long long passes = 0;       // passes of the last run
+    ~StreamPlan() { if (graph) cudaGraphExecDestroy(graph); }
+};
+
 struct as_solver {
     int device = 0;
     int precision = AS_PREC_F32_LOGA;
@@ -245,7 +258,8 @@ struct as_solver {
     int track_best = 0;
     int forced_bt = 0;
     int forced_cl = 0;     // CTAs per trajectory in global-storage mode (0 = automatic)
-    int storage_mode = 0;  // 0 automatic, 1 shared memory only, 2 global storage only
+    int storage_mode = 0;  // 0 automatic, 1 shared memory, 2 global storage, 3 stream
+    std::unique_ptr<StreamPlan> sp;  // streamed solver state
 
     // trajectories
     int num_traj = 0;
@@ -841,6 +855,241 @@ int record_solve(as_solver* s, cudaStream_t st) {
     return AS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Streamed solver (AS_STORAGE_STREAM, as_stream.cuh): host side
+// ---------------------------------------------------------------------------
+constexpr long long kStreamAutoElements = 1ll << 19;  // AS_STORAGE_AUTO: N + M from here on
+
+bool use_stream(const as_solver* s) {
+    if (s->storage_mode == 3) return true;
+    if (s->storage_mode != 0 || s->num_traj <= 0) return false;
+    for (int t = 0; t < s->num_traj; t++) {
+        const auto& q = s->problems[s->traj_problem[t]];
+        if ((long long)q.n + q.m < kStreamAutoElements) return false;
+    }
+    return true;
+}
+
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+size_t stream_group_bytes(const PackedProblem& q, size_t vbytes) {
+    const long long E = (long long)q.n + q.m;
+    return 6 * round256((size_t)E * kLanes * vbytes) + round256((size_t)(q.n + 1) * kLanes * vbytes) +
+           round256((size_t)(q.nslots + 1) * kLanes * vbytes);
+}
+
+template <typename T>
+StreamArgs<T> stream_args(as_solver* s, int g, const unsigned long long* deadline) {
+    StreamPlan& P = *s->sp;
+    const int p = P.gprob[g];
+    const auto& q = s->problems[p];
+    const size_t vb = round256((size_t)((long long)q.n + q.m) * kLanes * sizeof(T));
+    char* base = static_cast<char*>(P.vec.p) + P.goff[g];
+    StreamArgs<T> A;
+    A.I = s->pool.host_inst[p];
+    A.X = reinterpret_cast<T*>(base);
+    A.K1 = reinterpret_cast<T*>(base + vb);
+    A.K2 = reinterpret_cast<T*>(base + 2 * vb);
+    A.K3 = reinterpret_cast<T*>(base + 3 * vb);
+    A.K4 = reinterpret_cast<T*>(base + 4 * vb);
+    A.K5 = reinterpret_cast<T*>(base + 5 * vb);
+    A.SY = reinterpret_cast<T*>(base + 6 * vb);
+    A.CS = reinterpret_cast<T*>(base + 6 * vb + round256((size_t)(q.n + 1) * kLanes * sizeof(T)));
+    A.lanes = P.lanes.as<LaneState>() + (size_t)g * kLanes;
+    A.tickets = P.tickets.as<int>() + 2 * g;
+    A.active = P.active.as<int>() + g;
+    A.cand_bits = P.cand.as<uint32_t>() + P.gcand[g];
+    A.best_bits = s->track_best ? s->best_bits.as<uint32_t>() : nullptr;
+    A.unit_bits = s->unit_bits.as<long long>();
+    A.inst_solved = s->solved.as<int>();
+    A.deadline = deadline;
+    A.pidx = p;
+    A.S = 1;
+    A.batch = s->batch;
+    A.maxsteps = s->max_steps;
+    A.stop_on_first = s->stop_on_first;
+    A.eps = s->eps;
+    A.tmax = s->max_time;
+    return A;
+}
+
+// Units sorted by problem, groups of four lanes, device storage and lane states.
+int stream_plan(as_solver* s) {
+    const int num_traj = s->num_traj;
+    const auto& pi = s->traj_problem;
+    s->order.resize(num_traj);
+    for (int t = 0; t < num_traj; t++) s->order[t] = t;
+    std::stable_sort(s->order.begin(), s->order.end(), [&](int a, int b) { return pi[a] < pi[b]; });
+    if (!s->sp) s->sp.reset(new StreamPlan());
+    StreamPlan& P = *s->sp;
+    P.gprob.clear();
+    P.goff.clear();
+    P.gcand.clear();
+    std::vector<LaneState> lanes;
+    const size_t vbytes = s->precision == AS_PREC_F64 ? 8 : 4;
+    size_t total = 0, cand_words = 0;
+    for (int u = 0; u < num_traj;) {
+        const int p = pi[s->order[u]];
+        const auto& q = s->problems[p];
+        P.gprob.push_back(p);
+        P.goff.push_back(total);
+        P.gcand.push_back(cand_words);
+        total += stream_group_bytes(q, vbytes);
+        cand_words += (size_t)kLanes * ((q.n + 31) / 32);
+        for (int l = 0; l < kLanes; l++) {
+            LaneState L;
+            std::memset(&L, 0, sizeof(L));
+            L.h = L.h0 = L.hnext = 1e-9;  // CpuRungeKutta's first step (as solve_kernel)
+            L.viol = -1;
+            L.minviol = INT_MAX;
+            L.unit = -1;
+            L.status = -1;  // padding lane: never runs
+            if (u < num_traj && pi[s->order[u]] == p) {
+                L.unit = u;
+                if (0.0 < s->max_time && 0 < s->max_steps) {
+                    L.status = SAT_UNKNOWN;
+                    L.rhs = 1;  // k1 of the first step
+                } else {
+                    L.status = 0.0 >= s->max_time ? SAT_MAXTIME_REACHED : SAT_MAXITER_REACHED;
+                }
+                u++;
+            }
+            lanes.push_back(L);
+        }
+    }
+    P.ngroups = (int)P.gprob.size();
+    AS_CUDA(P.vec.alloc(std::max<size_t>(total, 256)));
+    AS_CUDA(P.lanes.alloc(sizeof(LaneState) * lanes.size()));
+    AS_CUDA(P.tickets.alloc(sizeof(int) * 2 * P.ngroups));
+    AS_CUDA(P.active.alloc(sizeof(int) * P.ngroups));
+    AS_CUDA(P.cand.alloc(sizeof(uint32_t) * std::max<size_t>(cand_words, 1)));
+    std::vector<int> act(P.ngroups, 0);
+    for (int g = 0; g < P.ngroups; g++)
+        for (int l = 0; l < kLanes; l++) act[g] += lanes[(size_t)g * kLanes + l].status == SAT_UNKNOWN;
+    std::vector<int> ui(num_traj);
+    std::vector<long long> us(num_traj), ub(num_traj);
+    for (int u = 0; u < num_traj; u++) {
+        ui[u] = pi[s->order[u]];
+        us[u] = s->traj_off[s->order[u]];
+        ub[u] = s->traj_bits[s->order[u]];
+    }
+    AS_CUDA(cudaMemcpy(P.lanes.p, lanes.data(), sizeof(LaneState) * lanes.size(), cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(P.active.p, act.data(), sizeof(int) * P.ngroups, cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemset(P.tickets.p, 0, sizeof(int) * 2 * P.ngroups));
+    AS_CUDA(cudaMemcpy(s->unit_inst.p, ui.data(), sizeof(int) * num_traj, cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(s->unit_state.p, us.data(), sizeof(long long) * num_traj, cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(s->unit_bits.p, ub.data(), sizeof(long long) * num_traj, cudaMemcpyHostToDevice));
+    return AS_OK;
+}
+
+// One pass (an RK attempt of every lane) of every group, in stream order.
+template <typename T, bool LOGA, int KMAX, bool EXACT>
+int stream_record_pass(as_solver* s, cudaStream_t st, const unsigned long long* deadline) {
+    StreamPlan& P = *s->sp;
+    constexpr int BT = 256;
+    const int sms = s->sm_count;
+    for (int g = 0; g < P.ngroups; g++) {
+        StreamArgs<T> A = stream_args<T>(s, g, deadline);
+        const int n = A.I.n, m = A.I.m;
+        const int gc = std::max(1, std::min((m + BT - 1) / BT, sms * 8));
+        const int gv = std::max(1, std::min((n + BT - 1) / BT, sms * 8));
+        for (int S = 1; S <= 6; S++) {
+            A.S = S;
+            stream_clause_kernel<T, LOGA, KMAX, EXACT><<<gc, BT, 0, st>>>(A);
+            stream_var_kernel<T, LOGA><<<gv, BT, 0, st>>>(A);
+        }
+        const int words = (n + 31) / 32;
+        const int nbw = s->track_best ? std::max(1, std::min((words + BT / 32 - 1) / (BT / 32), sms * 2)) : 0;
+        stream_post_kernel<T, KMAX, EXACT><<<gv + gc + nbw, BT, 0, st>>>(A, gv, gc);
+        s->last_bt = BT;
+        s->last_ctas = gc;
+        s->last_smem = 0;
+        s->last_occ = 0;
+    }
+    AS_CUDA(cudaGetLastError());
+    return AS_OK;
+}
+
+template <typename T, bool LOGA, int KMAX, bool EXACT>
+int stream_run(as_solver* s) {
+    StreamPlan& P = *s->sp;
+    cudaStream_t st = s->stream;
+    AS_CUDA(cudaMemsetAsync(s->solved.p, 0, s->solved.bytes, st));
+    const bool have_deadline = s->wall_budget > 0.0;
+    const unsigned long long* deadline = have_deadline ? s->deadline.as<unsigned long long>() : nullptr;
+    if (have_deadline) {
+        stamp_deadline_kernel<<<1, 1, 0, st>>>(s->deadline.as<unsigned long long>(),
+                                               (unsigned long long)(s->wall_budget * 1e9));
+        AS_CUDA(cudaGetLastError());
+    }
+    for (int g = 0; g < P.ngroups; g++) {
+        StreamArgs<T> A = stream_args<T>(s, g, deadline);
+        const long long E = (long long)A.I.n + A.I.m;
+        const int blocks = (int)std::max(1ll, std::min((E + 255) / 256, (long long)s->sm_count * 8));
+        stream_load_kernel<T, LOGA><<<blocks, 256, 0, st>>>(A, static_cast<const T*>(s->states.p),
+                                                            s->unit_state.as<long long>());
+    }
+    AS_CUDA(cudaGetLastError());
+    if (P.graph) { cudaGraphExecDestroy(P.graph); P.graph = nullptr; }
+    cudaGraph_t graph = nullptr;
+    AS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int r = stream_record_pass<T, LOGA, KMAX, EXACT>(s, st, deadline);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (r) { if (graph) cudaGraphDestroy(graph); return r; }
+    if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("stream graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&P.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("stream graph instantiate: ") + cudaGetErrorString(e));
+    // Passes until every lane has finished.  The device applies the status rules and
+    // the wall-clock deadline (at every attempt); the host only polls the active-lane
+    // counts between chunks of passes.
+    std::vector<int> act(P.ngroups);
+    P.passes = 0;
+    int chunk = 2;
+    while (true) {
+        for (int i = 0; i < chunk; i++) AS_CUDA(cudaGraphLaunch(P.graph, st));
+        P.passes += chunk;
+        AS_CUDA(cudaMemcpyAsync(act.data(), P.active.p, sizeof(int) * P.ngroups, cudaMemcpyDeviceToHost, st));
+        AS_CUDA(cudaStreamSynchronize(st));
+        bool any = false;
+        for (int a : act) any |= a != 0;
+        if (!any) break;
+        chunk = std::min(chunk * 2, 16);
+    }
+    for (int g = 0; g < P.ngroups; g++) {
+        StreamArgs<T> A = stream_args<T>(s, g, deadline);
+        const long long E = (long long)A.I.n + A.I.m;
+        const int blocks = (int)std::max(1ll, std::min((E + 255) / 256, (long long)s->sm_count * 8));
+        stream_store_kernel<T, LOGA><<<blocks, 256, 0, st>>>(A, static_cast<T*>(s->states.p),
+                                                             s->unit_state.as<long long>(),
+                                                             s->results.as<UnitResult>());
+    }
+    AS_CUDA(cudaGetLastError());
+    AS_CUDA(cudaStreamSynchronize(st));
+    return AS_OK;
+}
+
+int stream_solve(as_solver* s) {
+    int r = stream_plan(s);
+    if (r) return r;
+    bool all3 = true, all4 = true;
+    int kmax = 0;
+    for (int p : s->sp->gprob) {
+        kmax = std::max(kmax, s->problems[p].k);
+        all3 = all3 && s->problems[p].k == 3;
+        all4 = all4 && s->problems[p].k == 4;
+    }
+    if (kmax > 16) return fail(AS_ERR_UNSUPPORTED, "clause length > 16 is not supported");
+    if (s->precision == AS_PREC_F64) {
+        if (all3) return stream_run<double, false, 3, true>(s);
+        if (all4) return stream_run<double, false, 4, true>(s);
+        return stream_run<double, false, 16, false>(s);
+    }
+    if (all3) return stream_run<float, true, 3, true>(s);
+    if (all4) return stream_run<float, true, 4, true>(s);
+    return stream_run<float, true, 16, false>(s);
+}
+
 }  // namespace
 
 int32_t as_solver_set_states_f64(as_solver* s, const int32_t* pi, int32_t nt, const double* st) {
@@ -866,6 +1115,12 @@ int32_t as_solver_solve_async(as_solver* s, void* stream) {
     if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
     if (s->num_traj <= 0) return fail(AS_ERR_NO_PROBLEM, "no trajectories set (as_solver_set_states_*)");
     AS_CUDA(cudaSetDevice(s->device));
+    if (use_stream(s)) {  // host-driven passes: runs to completion on the solver's stream
+        if (stream && (cudaStream_t)stream != s->stream) AS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+        s->groups_dirty = true;
+        return stream_solve(s);
+    }
     if (s->groups_dirty) {
         int r = build_groups(s);
         if (r) return r;
@@ -979,7 +1234,7 @@ int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas
 
 int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode) {
     if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
-    if (mode < 0 || mode > 2) return fail(AS_ERR_BAD_INPUT, "storage mode must be 0, 1 or 2");
+    if (mode < 0 || mode > 3) return fail(AS_ERR_BAD_INPUT, "storage mode must be 0, 1, 2 or 3");
     s->storage_mode = mode;
     s->groups_dirty = true;
     s->invalidate();

@@ -194,12 +194,19 @@ int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas
  * clause count, at least four).  Used by the autotuner. */
 int32_t as_solver_force_threads(as_solver* s, int32_t threads);
 /* Where a trajectory lives while it is integrated (no reference counterpart):
- * AS_STORAGE_AUTO picks shared memory when the instance fits one SM and global
- * storage (a per-CTA slab in device memory) otherwise; the other two force one.
+ * AS_STORAGE_AUTO picks the streamed solver when every instance has N + M >= 2^19
+ * state elements, else shared memory when the instance fits one SM, else global
+ * storage (a per-CTA slab in device memory); the others force one.
+ * AS_STORAGE_STREAM: trajectories of an instance are grouped by four with their
+ * states interleaved in device memory, and every RK attempt runs as per-stage
+ * kernels over the whole GPU, replayed from a CUDA graph; each trajectory keeps its
+ * own step size and the reference's counters.  It is host driven: a solve returns
+ * when the run is over (as_solver_solve_async first waits for the caller's stream).
  * Solves fail with AS_ERR_UNSUPPORTED when a forced mode cannot hold an instance. */
 #define AS_STORAGE_AUTO 0
 #define AS_STORAGE_SHARED 1
 #define AS_STORAGE_GLOBAL 2
+#define AS_STORAGE_STREAM 3
 int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode);
 /* CTAs per trajectory in global-storage mode (no reference counterpart): 0 picks
  * automatically (a thread-block cluster of 4 or 8 CTAs when there are few
