@@ -235,6 +235,8 @@ struct StreamPlan {
     std::vector<size_t> goff;   // byte offset of each group's vectors in vec
     std::vector<size_t> gcand;  // word offset of each group's candidate assignments
     DevBuf vec, lanes, tickets, active, cand;
+    std::vector<std::unique_ptr<DevBuf>> vstart, vpos;  // per problem occurrence lists
+    std::vector<int> have_lists;
     cudaGraphExec_t graph = nullptr;
     long long passes = 0;       // passes of the last run
     ~StreamPlan() { if (graph) cudaGraphExecDestroy(graph); }
@@ -875,7 +877,7 @@ size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 size_t stream_group_bytes(const PackedProblem& q, size_t vbytes) {
     const long long E = (long long)q.n + q.m;
     return 6 * round256((size_t)E * kLanes * vbytes) + round256((size_t)(q.n + 1) * kLanes * vbytes) +
-           round256((size_t)(q.nslots + 1) * kLanes * vbytes);
+           round256((size_t)q.k * q.mp * kLanes * vbytes);
 }
 
 template <typename T>
@@ -896,6 +898,8 @@ StreamArgs<T> stream_args(as_solver* s, int g, const unsigned long long* deadlin
     A.SY = reinterpret_cast<T*>(base + 6 * vb);
     A.CS = reinterpret_cast<T*>(base + 6 * vb + round256((size_t)(q.n + 1) * kLanes * sizeof(T)));
     A.lanes = P.lanes.as<LaneState>() + (size_t)g * kLanes;
+    A.vstart = P.vstart[p]->as<int>();
+    A.vpos = P.vpos[p]->as<int>();
     A.tickets = P.tickets.as<int>() + 2 * g;
     A.active = P.active.as<int>() + g;
     A.cand_bits = P.cand.as<uint32_t>() + P.gcand[g];
@@ -911,6 +915,39 @@ StreamArgs<T> stream_args(as_solver* s, int g, const unsigned long long* deadlin
     A.eps = s->eps;
     A.tmax = s->max_time;
     return A;
+}
+
+// Occurrence lists of a packed problem's internal variables: the contribution rows
+// q * mp + m of its literals, in the order of its SELL row (public clause order).
+int stream_lists(as_solver* s, int p) {
+    StreamPlan& P = *s->sp;
+    const auto& q = s->problems[p];
+    std::vector<int> start(q.n + 1, 0), pos;
+    for (int v = 0; v < q.n; v++) start[v + 1] = start[v];
+    std::vector<int> deg(q.n, 0);
+    for (int qq = 0; qq < q.k; qq++)
+        for (int m = 0; m < q.m; m++) {
+            const uint32_t v = q.litw[(size_t)qq * q.mp + m] & 0x7fffffffu;
+            if ((int)v < q.n) deg[v]++;
+        }
+    for (int v = 0; v < q.n; v++) start[v + 1] = start[v] + deg[v];
+    pos.assign(std::max(start[q.n], 1), 0);
+    for (int qq = 0; qq < q.k; qq++)
+        for (int m = 0; m < q.m; m++) {
+            const size_t idx = (size_t)qq * q.mp + m;
+            const uint32_t v = q.litw[idx] & 0x7fffffffu;
+            if ((int)v >= q.n) continue;
+            const int rank = (int)(q.slotw[idx] >> 5) - q.srow[v >> 5];  // row in v's SELL list
+            pos[start[v] + rank] = (int)idx;
+        }
+    P.vstart[p].reset(new DevBuf());
+    P.vpos[p].reset(new DevBuf());
+    AS_CUDA(P.vstart[p]->alloc(sizeof(int) * start.size()));
+    AS_CUDA(P.vpos[p]->alloc(sizeof(int) * pos.size()));
+    AS_CUDA(cudaMemcpy(P.vstart[p]->p, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
+    AS_CUDA(cudaMemcpy(P.vpos[p]->p, pos.data(), sizeof(int) * pos.size(), cudaMemcpyHostToDevice));
+    P.have_lists[p] = 1;
+    return AS_OK;
 }
 
 // Units sorted by problem, groups of four lanes, device storage and lane states.
@@ -958,6 +995,17 @@ int stream_plan(as_solver* s) {
         }
     }
     P.ngroups = (int)P.gprob.size();
+    const size_t np = s->problems.size();
+    if (P.have_lists.size() != np) {
+        P.have_lists.assign(np, 0);
+        P.vstart.resize(np);
+        P.vpos.resize(np);
+    }
+    for (int p : P.gprob)
+        if (!P.have_lists[p]) {
+            int r = stream_lists(s, p);
+            if (r) return r;
+        }
     AS_CUDA(P.vec.alloc(std::max<size_t>(total, 256)));
     AS_CUDA(P.lanes.alloc(sizeof(LaneState) * lanes.size()));
     AS_CUDA(P.tickets.alloc(sizeof(int) * 2 * P.ngroups));
@@ -991,8 +1039,9 @@ int stream_record_pass(as_solver* s, cudaStream_t st, const unsigned long long* 
     for (int g = 0; g < P.ngroups; g++) {
         StreamArgs<T> A = stream_args<T>(s, g, deadline);
         const int n = A.I.n, m = A.I.m;
-        const int gc = std::max(1, std::min((m + BT - 1) / BT, sms * 8));
-        const int gv = std::max(1, std::min((n + BT - 1) / BT, sms * 8));
+        // two threads per clause / variable row in the stage kernels
+        const int gc = (int)std::max(1ll, std::min((2ll * m + BT - 1) / BT, (long long)sms * 8));
+        const int gv = (int)std::max(1ll, std::min((2ll * n + BT - 1) / BT, (long long)sms * 8));
         for (int S = 1; S <= 6; S++) {
             A.S = S;
             stream_clause_kernel<T, LOGA, KMAX, EXACT><<<gc, BT, 0, st>>>(A);
@@ -1000,7 +1049,9 @@ int stream_record_pass(as_solver* s, cudaStream_t st, const unsigned long long* 
         }
         const int words = (n + 31) / 32;
         const int nbw = s->track_best ? std::max(1, std::min((words + BT / 32 - 1) / (BT / 32), sms * 2)) : 0;
-        stream_post_kernel<T, KMAX, EXACT><<<gv + gc + nbw, BT, 0, st>>>(A, gv, gc);
+        const int pv = std::max(1, std::min((n + BT - 1) / BT, sms * 4));
+        const int pc = std::max(1, std::min((m + BT - 1) / BT, sms * 8));
+        stream_post_kernel<T, KMAX, EXACT><<<pv + pc + nbw, BT, 0, st>>>(A, pv, pc);
         s->last_bt = BT;
         s->last_ctas = gc;
         s->last_smem = 0;

@@ -5,18 +5,24 @@
 // SatSolver.h:273-355, AnalogSAT/cpu_sat/CpuRungeKutta.cpp:66-100,181-267,
 // AnalogSAT/cpu_sat/CpuSat.cpp:65-94,136-173,199-241), reorganised for the whole GPU:
 //
-//  * Trajectories of one instance are grouped by four ("lanes").  Every per-element
-//    vector of a group is stored interleaved, [element][lane], so one random spin
-//    gather fetches the four lanes' spins in one 16-byte (FP32) access and one pass
-//    over the literal words serves four trajectories.
+//  * Trajectories of one instance are grouped by eight ("lanes").  Every per-element
+//    vector of a group is stored interleaved, [element][lane], so an FP32 element row
+//    is one whole 32-byte sector: a random spin gather or a contribution access moves
+//    no byte it does not use, and one pass over the literal words serves eight
+//    trajectories.  Two adjacent threads share a row, four lanes each, which keeps
+//    a thread's registers at four lanes' worth.
 //  * A group's vectors live in HBM: state X, stage derivatives K1..K5 (K2 doubles as
 //    the candidate state xnew after stage 6), stage spins SY (+ the sentinel row n,
-//    pinned at -1) and the SELL contribution slots CS.
+//    pinned at -1) and the literal contributions CS, clause-major ([slot q][clause]),
+//    so the clause kernel writes whole lines: scattered 16-byte partial-sector writes
+//    (the SELL slot order of the shared-memory kernels) cost as much as the whole rest
+//    of a pass here.  The variable kernel gathers a variable's contributions through
+//    its occurrence list (CSR, public clause order: the reference's summation order).
 //  * One "pass" is one RK attempt of every lane: per stage S = 1..6 a clause kernel
 //    (stage input of the clause weights, spin gathers, K_m, contributions into CS,
 //    da -> K_S) and a variable kernel (SELL row sums -> K_S, spin input of stage S+1).
-//    The kernels are launched group by group, so a group's CS (4 x 4 B per slot) is
-//    written and read back while it is still in L2.
+//    The kernels are launched group by group, so a group's CS is written and read
+//    back while much of it is still in L2.
 //  * Each lane keeps its own step size, time, counters and status.  A lane whose
 //    previous attempt was rejected recomputes k1 at the same state (identical values)
 //    and retries with its smaller step; counters follow the reference (1 + 5 per
@@ -35,7 +41,8 @@
 
 namespace asb {
 
-constexpr int kLanes = 4;  // trajectories per stream group
+constexpr int kLanes = 8;  // trajectories per stream group: one 32-byte sector per FP32 element row
+constexpr int kSub = 4;    // lanes per thread in the clause and variable kernels (two threads per row)
 
 struct LaneState {
     double t, h, h0, hnext, hdid;
@@ -53,6 +60,8 @@ template <typename T>
 struct StreamArgs {
     DevInstance I;
     T *X, *K1, *K2, *K3, *K4, *K5, *SY, *CS;
+    const int* vstart;      // [n + 1] occurrence list offsets per internal variable
+    const int* vpos;        // occurrences: CS row q * mp + m, public clause order
     LaneState* lanes;       // [kLanes]
     int* tickets;           // [2] last-block tickets (decision, post)
     int* active;            // lanes of the group still running
@@ -65,7 +74,7 @@ struct StreamArgs {
     double eps, tmax;
 };
 
-template <typename T> struct L4 { T v[kLanes]; };
+template <typename T> struct L4 { T v[kSub]; };
 
 __device__ __forceinline__ L4<float> ld4(const float* p) {
     const float4 a = *reinterpret_cast<const float4*>(p);
@@ -83,20 +92,21 @@ __device__ __forceinline__ void st4(double* p, const L4<double>& a) {
     reinterpret_cast<double2*>(p)[1] = make_double2(a.v[2], a.v[3]);
 }
 
-// Per-lane block max of non-negative values, folded into lanes[l].err (atomicMax on
-// the bit pattern, which orders non-negative doubles like their values).
-__device__ __forceinline__ void lanes_max(const double (&v)[kLanes], double* red, LaneState* lanes) {
+// Per-lane block max of non-negative values, a thread holding kSub lanes starting at
+// lane (threadIdx.x & 1) * kSub, folded into lanes[l].err (atomicMax on the bit
+// pattern, which orders non-negative doubles like their values).
+__device__ __forceinline__ void lanes_max(const double (&v)[kSub], double* red, LaneState* lanes) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    double w[kLanes];
+    double w[kSub];
 #pragma unroll
-    for (int l = 0; l < kLanes; l++) {
+    for (int l = 0; l < kSub; l++) {
         w[l] = v[l];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) w[l] = fmax(w[l], __shfl_xor_sync(0xffffffffu, w[l], o));
+        for (int o = 2; o < 32; o <<= 1) w[l] = fmax(w[l], __shfl_xor_sync(0xffffffffu, w[l], o));
     }
-    if (lane == 0)
+    if (lane < 2)
 #pragma unroll
-        for (int l = 0; l < kLanes; l++) red[l * 32 + warp] = w[l];
+        for (int l = 0; l < kSub; l++) red[(lane * kSub + l) * 32 + warp] = w[l];
     __syncthreads();
     if (threadIdx.x < kLanes) {
         double m = 0.0;
@@ -117,9 +127,9 @@ __device__ __forceinline__ bool last_block(int* ticket, int* s_flag) {
 }
 
 template <typename T>
-__device__ __forceinline__ void load_lane_steps(const LaneState* L, T (&h)[kLanes], T (&h0)[kLanes]) {
+__device__ __forceinline__ void load_lane_steps(const LaneState* L, T (&h)[kSub], T (&h0)[kSub]) {
 #pragma unroll
-    for (int l = 0; l < kLanes; l++) {
+    for (int l = 0; l < kSub; l++) {
         h[l] = (T)L[l].h;
         h0[l] = (T)L[l].h0;
     }
@@ -142,19 +152,20 @@ __device__ __forceinline__ T stage_lane(int S, T x, T k1, T k2, T k3, T k4, T k5
 template <typename T>
 struct StageRow {
     L4<T> x, k1, k2, k3, k4, k5;
-    __device__ __forceinline__ void load(const StreamArgs<T>& A, long long r, int S) {
-        x = ld4(A.X + r * kLanes);
+    // i: index of the thread's first lane of the row ([row][lane] layout)
+    __device__ __forceinline__ void load(const StreamArgs<T>& A, long long i, int S) {
+        x = ld4(A.X + i);
         k1 = k2 = k3 = k4 = k5 = L4<T>{};
-        if (S >= 2) k1 = ld4(A.K1 + r * kLanes);
-        if (S >= 3) k2 = ld4(A.K2 + r * kLanes);
-        if (S >= 4) k3 = ld4(A.K3 + r * kLanes);
-        if (S >= 5) k4 = ld4(A.K4 + r * kLanes);
-        if (S >= 6) k5 = ld4(A.K5 + r * kLanes);
+        if (S >= 2) k1 = ld4(A.K1 + i);
+        if (S >= 3) k2 = ld4(A.K2 + i);
+        if (S >= 4) k3 = ld4(A.K3 + i);
+        if (S >= 5) k4 = ld4(A.K4 + i);
+        if (S >= 6) k5 = ld4(A.K5 + i);
     }
-    __device__ __forceinline__ L4<T> input(int S, const T (&h)[kLanes]) const {
+    __device__ __forceinline__ L4<T> input(int S, const T (&h)[kSub]) const {
         L4<T> y;
 #pragma unroll
-        for (int l = 0; l < kLanes; l++)
+        for (int l = 0; l < kSub; l++)
             y.v[l] = stage_lane<T>(S, x.v[l], k1.v[l], k2.v[l], k3.v[l], k4.v[l], k5.v[l], h[l]);
         return y;
     }
@@ -167,7 +178,8 @@ __device__ __forceinline__ T* stage_out(const StreamArgs<T>& A, int S) {
 
 // Stage S, clause side: a_m stage input, spin gathers, K_m and the leave-one-out
 // products (clause_phase's expression order, per lane), contributions into CS,
-// da_m -> K_S (stage 6: xnew -> K2 and the error ratio).
+// da_m -> K_S (stage 6: xnew -> K2 and the error ratio).  Two threads per clause,
+// kSub lanes each.
 template <typename T, bool LOGA, int KMAX, bool EXACT>
 __global__ void __launch_bounds__(256) stream_clause_kernel(StreamArgs<T> A) {
     using Ar = Arith<T>;
@@ -175,55 +187,59 @@ __global__ void __launch_bounds__(256) stream_clause_kernel(StreamArgs<T> A) {
     if (*A.active == 0) return;
     const DevInstance& I = A.I;
     const int S = A.S, n = I.n;
-    T h[kLanes], h0[kLanes];
-    load_lane_steps(A.lanes, h, h0);
+    const int lb = (threadIdx.x & 1) * kSub;  // first lane of this thread
+    T h[kSub], h0[kSub];
+    load_lane_steps(A.lanes + lb, h, h0);
     const T knorm = (T)ldexp(1.0, -I.k);
-    double em[kLanes] = {0.0, 0.0, 0.0, 0.0};
+    double em[kSub] = {0.0, 0.0, 0.0, 0.0};
     T* KS = stage_out(A, S);
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < I.m; m += gridDim.x * blockDim.x) {
-        const long long e = (long long)n + m;
+    const long long total = 2ll * I.m;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int m = (int)(it >> 1);
+        const long long i = ((long long)n + m) * kLanes + lb;
         StageRow<T> row;
-        row.load(A, e, S);
+        row.load(A, i, S);
         const L4<T> y = row.input(S, h);
         L4<T> am;
 #pragma unroll
-        for (int l = 0; l < kLanes; l++) {
+        for (int l = 0; l < kSub; l++) {
             if constexpr (LOGA) am.v[l] = exp2_fast(y.v[l]);
             else am.v[l] = y.v[l];
         }
         Lit<1> w[KMAX];
-        T f[KMAX][kLanes];
-        T km[kLanes];
+        T f[KMAX][kSub];
+        T km[kSub];
 #pragma unroll
-        for (int l = 0; l < kLanes; l++) km[l] = knorm;
+        for (int l = 0; l < kSub; l++) km[l] = knorm;
 #pragma unroll
         for (int q = 0; q < KMAX; q++) {
             if (EXACT || q < I.k) {
                 w[q].load(I, q * I.mp + m);
-                const L4<T> s = ld4(A.SY + (long long)w[q].var() * kLanes);
+                const L4<T> sv = ld4(A.SY + (long long)w[q].var() * kLanes + lb);
 #pragma unroll
-                for (int l = 0; l < kLanes; l++) {
-                    f[q][l] = w[q].neg() ? Ar::add(T(1), s.v[l]) : Ar::sub(T(1), s.v[l]);
+                for (int l = 0; l < kSub; l++) {
+                    f[q][l] = w[q].neg() ? Ar::add(T(1), sv.v[l]) : Ar::sub(T(1), sv.v[l]);
                     km[l] = Ar::mul(km[l], f[q][l]);
                 }
             }
         }
         L4<T> d;
 #pragma unroll
-        for (int l = 0; l < kLanes; l++) {
+        for (int l = 0; l < kSub; l++) {
             if constexpr (LOGA) d.v[l] = km[l] * km[l] * T(kInvLn2);
             else d.v[l] = Ar::mul(Ar::mul(am.v[l], km[l]), km[l]);
         }
         if (KMAX <= 10 || I.k <= 10) {
-            T r[kLanes];
+            T r[kSub];
 #pragma unroll
-            for (int l = 0; l < kLanes; l++) r[l] = Ar::mul(Ar::mul(km[l], knorm), am.v[l]);
+            for (int l = 0; l < kSub; l++) r[l] = Ar::mul(Ar::mul(km[l], knorm), am.v[l]);
 #pragma unroll
             for (int q = 0; q < KMAX; q++) {
                 if (EXACT || q < I.k) {
                     L4<T> c;
 #pragma unroll
-                    for (int l = 0; l < kLanes; l++) {
+                    for (int l = 0; l < kSub; l++) {
                         T prod = T(1);
                         bool first = true;
 #pragma unroll
@@ -237,7 +253,7 @@ __global__ void __launch_bounds__(256) stream_clause_kernel(StreamArgs<T> A) {
                         rr = rr + rr;
                         c.v[l] = w[q].neg() ? -rr : rr;
                     }
-                    st4(A.CS + (long long)w[q].slot() * kLanes, c);
+                    st4(A.CS + ((long long)q * I.mp + m) * kLanes + lb, c);
                 }
             }
         } else {
@@ -246,7 +262,7 @@ __global__ void __launch_bounds__(256) stream_clause_kernel(StreamArgs<T> A) {
                 if (EXACT || q < I.k) {
                     L4<T> c;
 #pragma unroll
-                    for (int l = 0; l < kLanes; l++) {
+                    for (int l = 0; l < kSub; l++) {
                         T temp = km[l];
 #pragma unroll
                         for (int j = 0; j < KMAX; j++)
@@ -254,21 +270,21 @@ __global__ void __launch_bounds__(256) stream_clause_kernel(StreamArgs<T> A) {
                         const T rr = Ar::mul(Ar::mul(Ar::mul(T(2), temp), knorm), am.v[l]);
                         c.v[l] = w[q].neg() ? -rr : rr;
                     }
-                    st4(A.CS + (long long)w[q].slot() * kLanes, c);
+                    st4(A.CS + ((long long)q * I.mp + m) * kLanes + lb, c);
                 }
             }
         }
         if (S < 6) {
-            st4(KS + e * kLanes, d);
+            st4(KS + i, d);
         } else {
             L4<T> xn;
 #pragma unroll
-            for (int l = 0; l < kLanes; l++) {
+            for (int l = 0; l < kSub; l++) {
                 em[l] = fmax(em[l], (double)rk_err_ratio(row.x.v[l], row.k1.v[l], row.k3.v[l], row.k4.v[l],
                                                          row.k5.v[l], d.v[l], h[l], h0[l], LOGA));
                 xn.v[l] = rk_new<T>(row.x.v[l], row.k1.v[l], row.k3.v[l], row.k4.v[l], d.v[l], h[l]);
             }
-            st4(A.K2 + e * kLanes, xn);
+            st4(A.K2 + i, xn);
         }
     }
     if (S == 6) lanes_max(em, red, A.lanes);
@@ -319,8 +335,9 @@ __device__ __forceinline__ void lane_decide(LaneState& L, const StreamArgs<T>& A
     }
 }
 
-// Stage S, variable side: SELL row sums -> K_S and the spin input of stage S + 1
-// (stage 6: xnew -> K2, the error ratio, and in the last block the lanes' decisions).
+// Stage S, variable side: occurrence-list sums -> K_S and the spin input of stage
+// S + 1 (stage 6: xnew -> K2, the error ratio, and in the last block the lanes'
+// decisions).  Two threads per variable, kSub lanes each.
 template <typename T, bool LOGA>
 __global__ void __launch_bounds__(256) stream_var_kernel(StreamArgs<T> A) {
     using Ar = Arith<T>;
@@ -329,43 +346,47 @@ __global__ void __launch_bounds__(256) stream_var_kernel(StreamArgs<T> A) {
     if (*A.active == 0) return;
     const DevInstance& I = A.I;
     const int S = A.S, n = I.n;
-    T h[kLanes], h0[kLanes];
-    load_lane_steps(A.lanes, h, h0);
-    double em[kLanes] = {0.0, 0.0, 0.0, 0.0};
+    const int lb = (threadIdx.x & 1) * kSub;
+    T h[kSub], h0[kSub];
+    load_lane_steps(A.lanes + lb, h, h0);
+    double em[kSub] = {0.0, 0.0, 0.0, 0.0};
     T* KS = stage_out(A, S);
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const int g = v >> 5;
-        const int r0 = ld_ro(I.srow + g), r1 = ld_ro(I.srow + g + 1);
+    const long long total = 2ll * n;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(it >> 1);
+        const long long i = (long long)v * kLanes + lb;
+        const int r0 = __ldg(A.vstart + v), r1 = __ldg(A.vstart + v + 1);
         L4<T> d;
 #pragma unroll
-        for (int l = 0; l < kLanes; l++) d.v[l] = T(0);
-        const T* p = A.CS + ((long long)r0 * 32 + (v & 31)) * kLanes;
-        for (int r = r0; r < r1; r++, p += 32 * kLanes) {
-            const L4<T> c = ld4(p);
+        for (int l = 0; l < kSub; l++) d.v[l] = T(0);
+#pragma unroll 8
+        for (int r = r0; r < r1; r++) {
+            const L4<T> c = ld4(A.CS + (long long)__ldg(A.vpos + r) * kLanes + lb);
 #pragma unroll
-            for (int l = 0; l < kLanes; l++) d.v[l] = Ar::add(d.v[l], c.v[l]);
+            for (int l = 0; l < kSub; l++) d.v[l] = Ar::add(d.v[l], c.v[l]);
         }
         StageRow<T> row;
         if (S < 6) {
-            st4(KS + (long long)v * kLanes, d);
+            st4(KS + i, d);
             // spin input of the next stage: K_S of this element was just formed
-            row.load(A, v, S);
+            row.load(A, i, S);
             if (S == 1) row.k1 = d;
             if (S == 2) row.k2 = d;
             if (S == 3) row.k3 = d;
             if (S == 4) row.k4 = d;
             if (S == 5) row.k5 = d;
-            st4(A.SY + (long long)v * kLanes, row.input(S + 1, h));
+            st4(A.SY + i, row.input(S + 1, h));
         } else {
-            row.load(A, v, 6);
+            row.load(A, i, 6);
             L4<T> xn;
 #pragma unroll
-            for (int l = 0; l < kLanes; l++) {
+            for (int l = 0; l < kSub; l++) {
                 em[l] = fmax(em[l], (double)rk_err_ratio(row.x.v[l], row.k1.v[l], row.k3.v[l], row.k4.v[l],
                                                          row.k5.v[l], d.v[l], h[l], h0[l], false));
                 xn.v[l] = rk_new<T>(row.x.v[l], row.k1.v[l], row.k3.v[l], row.k4.v[l], d.v[l], h[l]);
             }
-            st4(A.K2 + (long long)v * kLanes, xn);
+            st4(A.K2 + i, xn);
         }
     }
     if (S != 6) return;
@@ -387,61 +408,59 @@ __global__ void __launch_bounds__(256) stream_post_kernel(StreamArgs<T> A, int n
     if (*A.active == 0) return;
     const DevInstance& I = A.I;
     const int n = I.n, words = (n + 31) / 32;
-    int acc[kLanes], chk[kLanes];
-    bool any_acc = false, any_chk = false;
+    unsigned acc = 0, chk = 0;  // lane bit masks
 #pragma unroll
     for (int l = 0; l < kLanes; l++) {
-        acc[l] = A.lanes[l].acc;
-        chk[l] = A.lanes[l].check;
-        any_acc |= acc[l] != 0;
-        any_chk |= chk[l] != 0;
+        acc |= (A.lanes[l].acc ? 1u : 0u) << l;
+        chk |= (A.lanes[l].check ? 1u : 0u) << l;
     }
+    // commit of one element row: lanes whose attempt was accepted take K2
+    auto commit = [&](long long row) {
+#pragma unroll
+        for (int l = 0; l < kLanes; l++)
+            if ((acc >> l) & 1u) A.X[row * kLanes + l] = A.K2[row * kLanes + l];
+    };
     const int b = blockIdx.x;
     if (b < nbv) {
         for (int v = b * blockDim.x + threadIdx.x; v < n; v += nbv * blockDim.x) {
-            L4<T> x = ld4(A.X + (long long)v * kLanes);
-            if (any_acc) {
-                const L4<T> xn = ld4(A.K2 + (long long)v * kLanes);
+            T x[kLanes];
 #pragma unroll
-                for (int l = 0; l < kLanes; l++)
-                    if (acc[l]) x.v[l] = xn.v[l];
-                st4(A.X + (long long)v * kLanes, x);
+            for (int l = 0; l < kLanes; l++) {
+                x[l] = A.X[(long long)v * kLanes + l];
+                if ((acc >> l) & 1u) {
+                    x[l] = A.K2[(long long)v * kLanes + l];
+                    A.X[(long long)v * kLanes + l] = x[l];
+                }
+                A.SY[(long long)v * kLanes + l] = x[l];
             }
-            st4(A.SY + (long long)v * kLanes, x);
         }
     } else if (b < nbv + nbc) {
-        int cnt[kLanes] = {0, 0, 0, 0};
+        int cnt[kLanes];
+#pragma unroll
+        for (int l = 0; l < kLanes; l++) cnt[l] = 0;
         for (int m = (b - nbv) * blockDim.x + threadIdx.x; m < I.m; m += nbc * blockDim.x) {
             const long long e = (long long)n + m;
-            if (any_acc) {
-                L4<T> x = ld4(A.X + e * kLanes);
-                const L4<T> xn = ld4(A.K2 + e * kLanes);
-#pragma unroll
-                for (int l = 0; l < kLanes; l++)
-                    if (acc[l]) x.v[l] = xn.v[l];
-                st4(A.X + e * kLanes, x);
-            }
-            if (any_chk) {  // CpuSat::CalculateClauses on the accepted state (K2)
-                bool sat[kLanes] = {false, false, false, false};
+            if (acc) commit(e);
+            if (chk) {  // CpuSat::CalculateClauses on the accepted state (K2)
+                unsigned sat = 0;
 #pragma unroll
                 for (int q = 0; q < KMAX; q++) {
                     if (EXACT || q < I.k) {
                         Lit<1> w;
                         w.load(I, q * I.mp + m);
-                        const L4<T> s = w.var() < (uint32_t)n ? ld4(A.K2 + (long long)w.var() * kLanes)
-                                                              : L4<T>{{T(-1), T(-1), T(-1), T(-1)}};
 #pragma unroll
                         for (int l = 0; l < kLanes; l++) {
-                            const bool t = s.v[l] > T(0);
-                            sat[l] |= w.neg() ? !t : t;
+                            const T s = w.var() < (uint32_t)n ? A.K2[(long long)w.var() * kLanes + l] : T(-1);
+                            const bool t = s > T(0);
+                            sat |= ((w.neg() ? !t : t) ? 1u : 0u) << l;
                         }
                     }
                 }
 #pragma unroll
-                for (int l = 0; l < kLanes; l++) cnt[l] += sat[l] ? 0 : 1;
+                for (int l = 0; l < kLanes; l++) cnt[l] += ((sat >> l) & 1u) ? 0 : 1;
             }
         }
-        if (any_chk) {
+        if (chk) {
             const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
 #pragma unroll
             for (int l = 0; l < kLanes; l++) {
@@ -450,13 +469,13 @@ __global__ void __launch_bounds__(256) stream_post_kernel(StreamArgs<T> A, int n
                 if (lane == 0) red[l * 32 + warp] = cnt[l];
             }
             __syncthreads();
-            if (threadIdx.x < kLanes && chk[threadIdx.x]) {
-                int s = 0;
-                for (int i = 0; i < nw; i++) s += red[threadIdx.x * 32 + i];
-                atomicAdd(&A.lanes[threadIdx.x].vcount, s);
+            if (threadIdx.x < kLanes && ((chk >> threadIdx.x) & 1u)) {
+                int sum = 0;
+                for (int i = 0; i < nw; i++) sum += red[threadIdx.x * 32 + i];
+                atomicAdd(&A.lanes[threadIdx.x].vcount, sum);
             }
         }
-    } else if (any_chk && A.best_bits) {
+    } else if (chk && A.best_bits) {
         // assignment of lanes at a batch end, public variable order, one word per warp
         const int wpb = blockDim.x >> 5;
         const int nbw = gridDim.x - nbv - nbc;
@@ -464,11 +483,10 @@ __global__ void __launch_bounds__(256) stream_post_kernel(StreamArgs<T> A, int n
             const int i = wd * 32 + (threadIdx.x & 31);
             const bool in = i < n;
             const int v = in ? __ldg(I.iperm + i) : 0;
-            const L4<T> s = ld4(A.K2 + (long long)v * kLanes);
 #pragma unroll
             for (int l = 0; l < kLanes; l++) {
-                const unsigned bal = __ballot_sync(0xffffffffu, in && s.v[l] > T(0));
-                if (chk[l] && (threadIdx.x & 31) == 0) A.cand_bits[(long long)l * words + wd] = bal;
+                const unsigned bal = __ballot_sync(0xffffffffu, in && A.K2[(long long)v * kLanes + l] > T(0));
+                if (((chk >> l) & 1u) && (threadIdx.x & 31) == 0) A.cand_bits[(long long)l * words + wd] = bal;
             }
         }
     }
@@ -519,7 +537,7 @@ __global__ void __launch_bounds__(256) stream_post_kernel(StreamArgs<T> A, int n
 }
 
 // Initial state of a group: public states -> interleaved internal order (a -> log2 a),
-// stage-1 spins, zero contribution slots, sentinel spin row.
+// stage-1 spins, sentinel spin row.
 template <typename T, bool LOGA>
 __global__ void stream_load_kernel(StreamArgs<T> A, const T* __restrict__ states,
                                    const long long* __restrict__ unit_state) {
@@ -543,7 +561,6 @@ __global__ void stream_load_kernel(StreamArgs<T> A, const T* __restrict__ states
             else A.X[e * kLanes + l] = a;
         }
     }
-    for (long long r = tid; r < ((long long)I.nslots + 1) * kLanes; r += stride) A.CS[r] = T(0);
     if (tid < kLanes) A.SY[(long long)n * kLanes + tid] = T(-1);
 }
 

@@ -71,6 +71,8 @@ def parse_args():
                          "minimise unsat over --maxsat-seconds; adjoint: gradients of V at T=5 for "
                          "1024 random 3-SAT N=200, M=850 instances, FP32 vs FP64")
     ap.add_argument("--maxsat-seconds", type=float, default=60.0)
+    ap.add_argument("--maxsat-steps", type=int, default=0,
+                    help="maxsat workload: stop every trajectory after this many steps (0: budget only)")
     ap.add_argument("--max-steps", type=int, default=WORKLOAD["maxsteps"],
                     help="per-trajectory step cap (profiling runs use a small one)")
     return ap.parse_args()
@@ -496,7 +498,8 @@ def run_maxsat(args):
     lits, lens, _ = make_instance("fast", n, m, k, seed=5000)
     p = A.SatProblem.from_arrays(lits, lens)
     s = A.SatSolver([p])
-    s.SetEpsilon(1e-6); s.SetBatchSize(10); s.SetMaxSteps(10 ** 9); s.SetMaxTime(1e30)
+    steps = args.maxsat_steps if args.maxsat_steps > 0 else 10 ** 9
+    s.SetEpsilon(1e-6); s.SetBatchSize(min(10, steps)); s.SetMaxSteps(steps); s.SetMaxTime(1e30)
     s.SetTrackBest(True)
     s.SetWallBudget(args.maxsat_seconds)
     X = initial_states(n, m, T, seed=50_000, dtype=np.float32)
