@@ -241,9 +241,13 @@ class SatSolver:
         """CTAs per trajectory in global-storage mode: 0 automatic, 1, 4 or 8."""
         check(self._lib.as_solver_set_cluster_size(self._h, int(ctas)))
 
+    def SetStreamParts(self, parts: int):
+        """Clause parts per RK stage of the streamed solver (0: from the L2 budget)."""
+        check(self._lib.as_solver_set_stream_parts(self._h, int(parts)))
+
     def SetStorageMode(self, mode: int):
         """0 automatic, 1 shared memory only, 2 global storage (per-CTA slab) only,
-        3 streamed (four trajectories per lane group, per-stage kernels over the GPU)."""
+        3 streamed (eight trajectories per lane group, per-stage kernels over the GPU)."""
         check(self._lib.as_solver_set_storage_mode(self._h, int(mode)))
 
     # -- states (SatSolver::SetSatState, SatSolver.h:183-192) --

@@ -68,6 +68,7 @@ SIGNATURES = [
     ("as_solver_force_threads", _i32, [_vp, _i32]),
     ("as_solver_set_storage_mode", _i32, [_vp, _i32]),
     ("as_solver_set_cluster_size", _i32, [_vp, _i32]),
+    ("as_solver_set_stream_parts", _i32, [_vp, _i32]),
     ("as_solver_solve_noalloc", _i32, [_vp, _i32, _i32, _vp, _vp, _vp]),
     ("as_solver_adjoint", _i32, [_vp, C.c_double, _i32, _vp, _vp, _vp, _vp, _vp, _vp]),
 ]

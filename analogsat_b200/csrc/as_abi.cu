@@ -236,7 +236,7 @@ struct StreamPlan {
     std::vector<size_t> gcand;  // word offset of each group's candidate assignments
     DevBuf vec, lanes, tickets, active, cand;
     std::vector<std::unique_ptr<DevBuf>> vstart, vpos;  // per problem occurrence lists
-    std::vector<int> have_lists;
+    std::vector<int> have_lists, nparts;                // per problem clause parts
     cudaGraphExec_t graph = nullptr;
     long long passes = 0;       // passes of the last run
     ~StreamPlan() { if (graph) cudaGraphExecDestroy(graph); }
@@ -262,6 +262,7 @@ struct as_solver {
     int forced_cl = 0;     // CTAs per trajectory in global-storage mode (0 = automatic)
     int storage_mode = 0;  // 0 automatic, 1 shared memory, 2 global storage, 3 stream
     std::unique_ptr<StreamPlan> sp;  // streamed solver state
+    int stream_parts = 0;            // clause parts per stream pass (0 = from the L2 budget)
 
     // trajectories
     int num_traj = 0;
@@ -877,7 +878,7 @@ size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 size_t stream_group_bytes(const PackedProblem& q, size_t vbytes) {
     const long long E = (long long)q.n + q.m;
     return 6 * round256((size_t)E * kLanes * vbytes) + round256((size_t)(q.n + 1) * kLanes * vbytes) +
-           round256((size_t)q.k * q.mp * kLanes * vbytes);
+           round256((size_t)q.k * q.mp * kLanes * vbytes) + round256((size_t)q.n * kLanes * vbytes);
 }
 
 template <typename T>
@@ -900,6 +901,12 @@ StreamArgs<T> stream_args(as_solver* s, int g, const unsigned long long* deadlin
     A.lanes = P.lanes.as<LaneState>() + (size_t)g * kLanes;
     A.vstart = P.vstart[p]->as<int>();
     A.vpos = P.vpos[p]->as<int>();
+    A.ACC = reinterpret_cast<T*>(base + 6 * vb + round256((size_t)(q.n + 1) * kLanes * sizeof(T)) +
+                                 round256((size_t)q.k * q.mp * kLanes * sizeof(T)));
+    A.m0 = 0;
+    A.m1 = q.m;
+    A.part = 0;
+    A.nparts = P.nparts[p];
     A.tickets = P.tickets.as<int>() + 2 * g;
     A.active = P.active.as<int>() + g;
     A.cand_bits = P.cand.as<uint32_t>() + P.gcand[g];
@@ -917,21 +924,31 @@ StreamArgs<T> stream_args(as_solver* s, int g, const unsigned long long* deadlin
     return A;
 }
 
+
 // Occurrence lists of a packed problem's internal variables: the contribution rows
-// q * mp + m of its literals, in the order of its SELL row (public clause order).
+// q * mp + m of its literals, in the order of its SELL row (public clause order), and
+// their split into clause parts.  Parts are ranges of public clause index; they need
+// internal clause order = public order (the wide packing keeps it), else one part.
+// vstart holds nparts + 1 arrays of n offsets: part p of variable v is
+// [vstart[p n + v], vstart[(p + 1) n + v]).
 int stream_lists(as_solver* s, int p) {
     StreamPlan& P = *s->sp;
     const auto& q = s->problems[p];
-    std::vector<int> start(q.n + 1, 0), pos;
-    for (int v = 0; v < q.n; v++) start[v + 1] = start[v];
-    std::vector<int> deg(q.n, 0);
+    bool identity = true;
+    for (int m = 0; m < q.m && identity; m++) identity = q.cperm[m] == m;
+    // One part unless forced: on B200 at N = 1e5, M = 1e6 (CS 128 MB per group) the
+    // split did not pay -- 57.5k RHS/s in one part, 51.0k in two, 43.9k in four: the
+    // extra launches cost more than the L2 hits save.
+    int parts = 1;
+    if (identity && s->stream_parts > 0) parts = std::min(s->stream_parts, std::max(1, q.m));
+    std::vector<int> start(q.n + 1, 0), deg(q.n, 0);
     for (int qq = 0; qq < q.k; qq++)
         for (int m = 0; m < q.m; m++) {
             const uint32_t v = q.litw[(size_t)qq * q.mp + m] & 0x7fffffffu;
             if ((int)v < q.n) deg[v]++;
         }
     for (int v = 0; v < q.n; v++) start[v + 1] = start[v] + deg[v];
-    pos.assign(std::max(start[q.n], 1), 0);
+    std::vector<int> pos(std::max(start[q.n], 1), 0);
     for (int qq = 0; qq < q.k; qq++)
         for (int m = 0; m < q.m; m++) {
             const size_t idx = (size_t)qq * q.mp + m;
@@ -940,12 +957,24 @@ int stream_lists(as_solver* s, int p) {
             const int rank = (int)(q.slotw[idx] >> 5) - q.srow[v >> 5];  // row in v's SELL list
             pos[start[v] + rank] = (int)idx;
         }
+    std::vector<int> split((size_t)(parts + 1) * q.n);
+    for (int v = 0; v < q.n; v++) {
+        int r = start[v];
+        for (int pp = 0; pp < parts; pp++) {
+            split[(size_t)pp * q.n + v] = r;
+            const long long m1 = (long long)q.m * (pp + 1) / parts;
+            while (r < start[v + 1] && (pos[r] % q.mp) < m1) r++;
+        }
+        split[(size_t)parts * q.n + v] = start[v + 1];
+    }
     P.vstart[p].reset(new DevBuf());
     P.vpos[p].reset(new DevBuf());
-    AS_CUDA(P.vstart[p]->alloc(sizeof(int) * start.size()));
+    AS_CUDA(P.vstart[p]->alloc(sizeof(int) * std::max<size_t>(split.size(), 1)));
     AS_CUDA(P.vpos[p]->alloc(sizeof(int) * pos.size()));
-    AS_CUDA(cudaMemcpy(P.vstart[p]->p, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
+    if (!split.empty())
+        AS_CUDA(cudaMemcpy(P.vstart[p]->p, split.data(), sizeof(int) * split.size(), cudaMemcpyHostToDevice));
     AS_CUDA(cudaMemcpy(P.vpos[p]->p, pos.data(), sizeof(int) * pos.size(), cudaMemcpyHostToDevice));
+    P.nparts[p] = parts;
     P.have_lists[p] = 1;
     return AS_OK;
 }
@@ -998,6 +1027,7 @@ int stream_plan(as_solver* s) {
     const size_t np = s->problems.size();
     if (P.have_lists.size() != np) {
         P.have_lists.assign(np, 0);
+        P.nparts.assign(np, 1);
         P.vstart.resize(np);
         P.vpos.resize(np);
     }
@@ -1039,14 +1069,25 @@ int stream_record_pass(as_solver* s, cudaStream_t st, const unsigned long long* 
     for (int g = 0; g < P.ngroups; g++) {
         StreamArgs<T> A = stream_args<T>(s, g, deadline);
         const int n = A.I.n, m = A.I.m;
-        // two threads per clause / variable row in the stage kernels
-        const int gc = (int)std::max(1ll, std::min((2ll * m + BT - 1) / BT, (long long)sms * 8));
-        const int gv = (int)std::max(1ll, std::min((2ll * n + BT - 1) / BT, (long long)sms * 8));
+        // kRowThreads threads per clause / variable row in the stage kernels
+        const int gc = (int)std::max(1ll, std::min(((long long)kRowThreads * m + BT - 1) / BT, (long long)sms * 8));
+        const int gv = (int)std::max(1ll, std::min(((long long)kRowThreads * n + BT - 1) / BT, (long long)sms * 8));
+        const int* vstart0 = A.vstart;
         for (int S = 1; S <= 6; S++) {
             A.S = S;
-            stream_clause_kernel<T, LOGA, KMAX, EXACT><<<gc, BT, 0, st>>>(A);
-            stream_var_kernel<T, LOGA><<<gv, BT, 0, st>>>(A);
+            for (int part = 0; part < A.nparts; part++) {
+                A.part = part;
+                A.m0 = (int)((long long)m * part / A.nparts);
+                A.m1 = (int)((long long)m * (part + 1) / A.nparts);
+                A.vstart = vstart0 + (size_t)part * n;
+                const int gcp = (int)std::max(1ll, std::min(((long long)kRowThreads * (A.m1 - A.m0) + BT - 1) / BT,
+                                                            (long long)sms * 8));
+                stream_clause_kernel<T, LOGA, KMAX, EXACT><<<gcp, BT, 0, st>>>(A);
+                stream_var_kernel<T, LOGA><<<gv, BT, 0, st>>>(A);
+            }
         }
+        A.vstart = vstart0;
+        A.part = 0;
         const int words = (n + 31) / 32;
         const int nbw = s->track_best ? std::max(1, std::min((words + BT / 32 - 1) / (BT / 32), sms * 2)) : 0;
         const int pv = std::max(1, std::min((n + BT - 1) / BT, sms * 4));
@@ -1289,6 +1330,14 @@ int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode) {
     s->storage_mode = mode;
     s->groups_dirty = true;
     s->invalidate();
+    return AS_OK;
+}
+
+int32_t as_solver_set_stream_parts(as_solver* s, int32_t parts) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (parts < 0 || parts > 8) return fail(AS_ERR_BAD_INPUT, "stream parts must be 0 (automatic) to 8");
+    s->stream_parts = parts;
+    if (s->sp) s->sp->have_lists.clear();
     return AS_OK;
 }
 

@@ -20,7 +20,11 @@
 //    its occurrence list (CSR, public clause order: the reference's summation order).
 //  * One "pass" is one RK attempt of every lane: per stage S = 1..6 a clause kernel
 //    (stage input of the clause weights, spin gathers, K_m, contributions into CS,
-//    da -> K_S) and a variable kernel (SELL row sums -> K_S, spin input of stage S+1).
+//    da -> K_S) and a variable kernel (occurrence-list sums -> K_S, spin input of
+//    stage S+1).  Optionally (as_solver_set_stream_parts) the clauses are split into
+//    parts by public index, each part's clause kernel followed at once by a variable
+//    kernel that continues the row sums over that part's occurrences (the sums still
+//    run in public clause order), so CS is read back from L2.
 //    The kernels are launched group by group, so a group's CS is written and read
 //    back while much of it is still in L2.
 //  * Each lane keeps its own step size, time, counters and status.  A lane whose
@@ -41,8 +45,13 @@
 
 namespace asb {
 
-constexpr int kLanes = 8;  // trajectories per stream group: one 32-byte sector per FP32 element row
-constexpr int kSub = 4;    // lanes per thread in the clause and variable kernels (two threads per row)
+#ifndef AS_STREAM_LANES
+#define AS_STREAM_LANES 8
+#endif
+constexpr int kLanes = AS_STREAM_LANES;  // trajectories per stream group
+constexpr int kSub = 4;                  // lanes per thread in the clause and variable kernels
+constexpr int kRowThreads = kLanes / kSub;  // threads sharing an element row
+static_assert(kLanes % kSub == 0 && kRowThreads <= 32 && (kRowThreads & (kRowThreads - 1)) == 0, "lane split");
 
 struct LaneState {
     double t, h, h0, hnext, hdid;
@@ -60,8 +69,11 @@ template <typename T>
 struct StreamArgs {
     DevInstance I;
     T *X, *K1, *K2, *K3, *K4, *K5, *SY, *CS;
-    const int* vstart;      // [n + 1] occurrence list offsets per internal variable
+    T* ACC;                 // [n][kLanes] partial row sums between clause parts
+    const int* vstart;      // this part's occurrence ranges: [vstart[v], vstart[n + v])
     const int* vpos;        // occurrences: CS row q * mp + m, public clause order
+    int m0, m1;             // clause range of this part
+    int part, nparts;
     LaneState* lanes;       // [kLanes]
     int* tickets;           // [2] last-block tickets (decision, post)
     int* active;            // lanes of the group still running
@@ -93,7 +105,7 @@ __device__ __forceinline__ void st4(double* p, const L4<double>& a) {
 }
 
 // Per-lane block max of non-negative values, a thread holding kSub lanes starting at
-// lane (threadIdx.x & 1) * kSub, folded into lanes[l].err (atomicMax on the bit
+// lane (threadIdx.x % kRowThreads) * kSub, folded into lanes[l].err (atomicMax on the bit
 // pattern, which orders non-negative doubles like their values).
 __device__ __forceinline__ void lanes_max(const double (&v)[kSub], double* red, LaneState* lanes) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -102,9 +114,9 @@ __device__ __forceinline__ void lanes_max(const double (&v)[kSub], double* red, 
     for (int l = 0; l < kSub; l++) {
         w[l] = v[l];
 #pragma unroll
-        for (int o = 2; o < 32; o <<= 1) w[l] = fmax(w[l], __shfl_xor_sync(0xffffffffu, w[l], o));
+        for (int o = kRowThreads; o < 32; o <<= 1) w[l] = fmax(w[l], __shfl_xor_sync(0xffffffffu, w[l], o));
     }
-    if (lane < 2)
+    if (lane < kRowThreads)
 #pragma unroll
         for (int l = 0; l < kSub; l++) red[(lane * kSub + l) * 32 + warp] = w[l];
     __syncthreads();
@@ -178,8 +190,8 @@ __device__ __forceinline__ T* stage_out(const StreamArgs<T>& A, int S) {
 
 // Stage S, clause side: a_m stage input, spin gathers, K_m and the leave-one-out
 // products (clause_phase's expression order, per lane), contributions into CS,
-// da_m -> K_S (stage 6: xnew -> K2 and the error ratio).  Two threads per clause,
-// kSub lanes each.
+// da_m -> K_S (stage 6: xnew -> K2 and the error ratio).  kRowThreads threads per
+// clause, kSub lanes each.
 template <typename T, bool LOGA, int KMAX, bool EXACT>
 __global__ void __launch_bounds__(256) stream_clause_kernel(StreamArgs<T> A) {
     using Ar = Arith<T>;
@@ -187,16 +199,16 @@ __global__ void __launch_bounds__(256) stream_clause_kernel(StreamArgs<T> A) {
     if (*A.active == 0) return;
     const DevInstance& I = A.I;
     const int S = A.S, n = I.n;
-    const int lb = (threadIdx.x & 1) * kSub;  // first lane of this thread
+    const int lb = (threadIdx.x % kRowThreads) * kSub;  // first lane of this thread
     T h[kSub], h0[kSub];
     load_lane_steps(A.lanes + lb, h, h0);
     const T knorm = (T)ldexp(1.0, -I.k);
     double em[kSub] = {0.0, 0.0, 0.0, 0.0};
     T* KS = stage_out(A, S);
-    const long long total = 2ll * I.m;
+    const long long total = (long long)kRowThreads * (A.m1 - A.m0);
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
          it += (long long)gridDim.x * blockDim.x) {
-        const int m = (int)(it >> 1);
+        const int m = A.m0 + (int)(it / kRowThreads);
         const long long i = ((long long)n + m) * kLanes + lb;
         StageRow<T> row;
         row.load(A, i, S);
@@ -337,7 +349,7 @@ __device__ __forceinline__ void lane_decide(LaneState& L, const StreamArgs<T>& A
 
 // Stage S, variable side: occurrence-list sums -> K_S and the spin input of stage
 // S + 1 (stage 6: xnew -> K2, the error ratio, and in the last block the lanes'
-// decisions).  Two threads per variable, kSub lanes each.
+// decisions).  kRowThreads threads per variable, kSub lanes each.
 template <typename T, bool LOGA>
 __global__ void __launch_bounds__(256) stream_var_kernel(StreamArgs<T> A) {
     using Ar = Arith<T>;
@@ -346,25 +358,33 @@ __global__ void __launch_bounds__(256) stream_var_kernel(StreamArgs<T> A) {
     if (*A.active == 0) return;
     const DevInstance& I = A.I;
     const int S = A.S, n = I.n;
-    const int lb = (threadIdx.x & 1) * kSub;
+    const int lb = (threadIdx.x % kRowThreads) * kSub;
     T h[kSub], h0[kSub];
     load_lane_steps(A.lanes + lb, h, h0);
     double em[kSub] = {0.0, 0.0, 0.0, 0.0};
     T* KS = stage_out(A, S);
-    const long long total = 2ll * n;
+    const long long total = (long long)kRowThreads * n;
     for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < total;
          it += (long long)gridDim.x * blockDim.x) {
-        const int v = (int)(it >> 1);
+        const int v = (int)(it / kRowThreads);
         const long long i = (long long)v * kLanes + lb;
-        const int r0 = __ldg(A.vstart + v), r1 = __ldg(A.vstart + v + 1);
+        const int r0 = __ldg(A.vstart + v), r1 = __ldg(A.vstart + n + v);
         L4<T> d;
+        if (A.part > 0) {
+            d = ld4(A.ACC + i);  // the sum so far, continued in the same order
+        } else {
 #pragma unroll
-        for (int l = 0; l < kSub; l++) d.v[l] = T(0);
+            for (int l = 0; l < kSub; l++) d.v[l] = T(0);
+        }
 #pragma unroll 8
         for (int r = r0; r < r1; r++) {
             const L4<T> c = ld4(A.CS + (long long)__ldg(A.vpos + r) * kLanes + lb);
 #pragma unroll
             for (int l = 0; l < kSub; l++) d.v[l] = Ar::add(d.v[l], c.v[l]);
+        }
+        if (A.part + 1 < A.nparts) {
+            st4(A.ACC + i, d);
+            continue;
         }
         StageRow<T> row;
         if (S < 6) {
@@ -389,7 +409,7 @@ __global__ void __launch_bounds__(256) stream_var_kernel(StreamArgs<T> A) {
             st4(A.K2 + i, xn);
         }
     }
-    if (S != 6) return;
+    if (S != 6 || A.part + 1 < A.nparts) return;
     lanes_max(em, red, A.lanes);
     if (!last_block(A.tickets, &s_flag)) return;
     if (threadIdx.x < kLanes) lane_decide(A.lanes[threadIdx.x], A);

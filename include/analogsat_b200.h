@@ -208,6 +208,13 @@ int32_t as_solver_force_threads(as_solver* s, int32_t threads);
 #define AS_STORAGE_GLOBAL 2
 #define AS_STORAGE_STREAM 3
 int32_t as_solver_set_storage_mode(as_solver* s, int32_t mode);
+/* Clause parts per RK stage in AS_STORAGE_STREAM (no reference counterpart): the
+ * clauses of an instance whose internal order is the public one (the wide packing)
+ * are split into this many ranges, each range's contributions summed right after it
+ * is computed (while still in L2), the row sums continuing from range to range in
+ * public clause order.  0 (default) and 1: one range; up to 8.  Results do not depend
+ * on it. */
+int32_t as_solver_set_stream_parts(as_solver* s, int32_t parts);
 /* CTAs per trajectory in global-storage mode (no reference counterpart): 0 picks
  * automatically (a thread-block cluster of 4 or 8 CTAs when there are few
  * trajectories, so that they still cover the whole GPU), 1, 4 or 8 force it. */

@@ -72,6 +72,27 @@ def test_stream_f64_matches_shared_memory_solver_golden(golden, tag):
           _run([p, q], 1, pidx, ics, 3, batch=5, maxsteps=120))
 
 
+@pytest.mark.parametrize("parts", [1, 3])
+def test_stream_f64_wide_instance_matches_global_storage(parts):
+    """N=6000, M=25500 (wide literal words, public clause order): the stream solver,
+    with its clauses in one part or split into three parts whose row sums continue
+    from part to part, against the global-storage solver, bit for bit."""
+    from analogsat_b200 import SatProblem
+    from analogsat_b200.instances import make_instance, initial_states
+    n, m, T = 6000, 25500, 5
+    lits, lens, _ = make_instance("planted", n, m, 3, seed=8)
+    p = SatProblem.from_arrays(lits, lens)
+    assert not p.layout_stats(1)["compact"]
+    ics = initial_states(n, m, T, seed=5)
+    ref = _run([p], 1, np.zeros(T), ics, 2, batch=6, maxsteps=60)
+    s = _solver([p], 1, batch=6, maxsteps=60)
+    s.SetStorageMode(3)
+    s.SetStreamParts(parts)
+    s.SetSatStates(np.zeros(T, np.int32), ics)
+    s.Solve()
+    _same(ref, (s.results(), s.GetSatStates(np.float64)))
+
+
 def test_stream_f32_short_horizon_error(oracle):
     """FP32 stream lanes against the FP64 solution of the ODE at the same time."""
     from analogsat_b200 import SatProblem
