@@ -434,25 +434,29 @@ __global__ void __launch_bounds__(256) stream_post_kernel(StreamArgs<T> A, int n
         acc |= (A.lanes[l].acc ? 1u : 0u) << l;
         chk |= (A.lanes[l].check ? 1u : 0u) << l;
     }
-    // commit of one element row: lanes whose attempt was accepted take K2
-    auto commit = [&](long long row) {
+    // commit of one element row (vector accesses, kSub lanes each): lanes whose
+    // attempt was accepted take K2; the committed row is returned in x
+    auto commit = [&](long long row, L4<T> (&x)[kRowThreads]) {
 #pragma unroll
-        for (int l = 0; l < kLanes; l++)
-            if ((acc >> l) & 1u) A.X[row * kLanes + l] = A.K2[row * kLanes + l];
+        for (int c = 0; c < kRowThreads; c++) {
+            const long long i = row * kLanes + c * kSub;
+            x[c] = ld4(A.X + i);
+            if ((acc >> (c * kSub)) & ((1u << kSub) - 1u)) {
+                const L4<T> xn = ld4(A.K2 + i);
+#pragma unroll
+                for (int l = 0; l < kSub; l++)
+                    if ((acc >> (c * kSub + l)) & 1u) x[c].v[l] = xn.v[l];
+                st4(A.X + i, x[c]);
+            }
+        }
     };
     const int b = blockIdx.x;
     if (b < nbv) {
         for (int v = b * blockDim.x + threadIdx.x; v < n; v += nbv * blockDim.x) {
-            T x[kLanes];
+            L4<T> x[kRowThreads];
+            commit(v, x);
 #pragma unroll
-            for (int l = 0; l < kLanes; l++) {
-                x[l] = A.X[(long long)v * kLanes + l];
-                if ((acc >> l) & 1u) {
-                    x[l] = A.K2[(long long)v * kLanes + l];
-                    A.X[(long long)v * kLanes + l] = x[l];
-                }
-                A.SY[(long long)v * kLanes + l] = x[l];
-            }
+            for (int c = 0; c < kRowThreads; c++) st4(A.SY + (long long)v * kLanes + c * kSub, x[c]);
         }
     } else if (b < nbv + nbc) {
         int cnt[kLanes];
@@ -460,7 +464,10 @@ __global__ void __launch_bounds__(256) stream_post_kernel(StreamArgs<T> A, int n
         for (int l = 0; l < kLanes; l++) cnt[l] = 0;
         for (int m = (b - nbv) * blockDim.x + threadIdx.x; m < I.m; m += nbc * blockDim.x) {
             const long long e = (long long)n + m;
-            if (acc) commit(e);
+            if (acc) {
+                L4<T> x[kRowThreads];
+                commit(e, x);
+            }
             if (chk) {  // CpuSat::CalculateClauses on the accepted state (K2)
                 unsigned sat = 0;
 #pragma unroll
@@ -468,11 +475,16 @@ __global__ void __launch_bounds__(256) stream_post_kernel(StreamArgs<T> A, int n
                     if (EXACT || q < I.k) {
                         Lit<1> w;
                         w.load(I, q * I.mp + m);
+                        const bool real = w.var() < (uint32_t)n;
 #pragma unroll
-                        for (int l = 0; l < kLanes; l++) {
-                            const T s = w.var() < (uint32_t)n ? A.K2[(long long)w.var() * kLanes + l] : T(-1);
-                            const bool t = s > T(0);
-                            sat |= ((w.neg() ? !t : t) ? 1u : 0u) << l;
+                        for (int c = 0; c < kRowThreads; c++) {
+                            const L4<T> sv = real ? ld4(A.K2 + (long long)w.var() * kLanes + c * kSub)
+                                                  : L4<T>{{T(-1), T(-1), T(-1), T(-1)}};
+#pragma unroll
+                            for (int l = 0; l < kSub; l++) {
+                                const bool t = sv.v[l] > T(0);
+                                sat |= ((w.neg() ? !t : t) ? 1u : 0u) << (c * kSub + l);
+                            }
                         }
                     }
                 }
