@@ -515,10 +515,24 @@ def run_maxsat(args):
         best = s.GetBestAssignment(t)
         exact.append(int((~np.where(c > 0, best[v], ~best[v]).any(axis=1)).sum()))
     assert exact == list(r["min_violations"]), "device min-unsat disagrees with the host recount"
+    rhs_s = float(r["rhs"].sum()) / wall
+    try:
+        hbm_peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    except OSError:
+        hbm_peak = 6650.0
+    # streamed mode, eight trajectories per lane group: the literal words are read once
+    # per group and RHS, so B_rhs = 8(N+M) + 4KM/8 per trajectory and RHS
+    b_rhs = 8 * (n + m) + 4 * k * m / 8
     print(json.dumps({"workload": "maxsat-random-4sat-N1e5-M1e6-x32-traj", "wall_s": wall,
                       "budget_s": args.maxsat_seconds, "min_unsat": int(min(exact)),
                       "median_min_unsat": float(np.median(exact)), "steps_median": float(np.median(r["steps"])),
-                      "rhs_evals_per_s": float(r["rhs"].sum()) / wall,
+                      "rhs_evals_per_s": rhs_s,
+                      "roofline": {"bound": "hbm", "achieved": rhs_s * b_rhs / 1e9, "peak": hbm_peak,
+                                   "unit": "GB/s", "frac": rhs_s * b_rhs / 1e9 / hbm_peak,
+                                   "note": "achieved = RHS/s x B_rhs (T_share 8); the stage vectors of the "
+                                           "clause weights and the contribution intermediate are extra HBM "
+                                           "traffic B_rhs leaves out (~12 GB per pass of 192 RHS, "
+                                           "profiles/stream_kernels_maxsat_N1e5_M1e6.md)"},
                       "launch_shape": s.launch_shape()}), flush=True)
 
 
