@@ -126,6 +126,26 @@ class SatProblem:
         check(self._lib.as_problem_get_clauses(self._h, _ptr(lits), _ptr(lens)))
         return lits[:nl], lens[: self.m]
 
+    def set_model(self, tanh: bool = False, q: float = 1.1):
+        """The reference's choice of CTDS class: CpuSat (tanh=False) or CpuSatTanh with
+        slope q (Set_Q).  Device RHS calls and solvers created afterwards use it."""
+        check(self._lib.as_problem_set_model(self._h, _abi.AS_MODEL_TANH if tanh else _abi.AS_MODEL_CTDS,
+                                             float(q)))
+        return self
+
+    def set_bias(self, b: float):
+        """ISat::Set_B: the bias term mean(a) (M/N) b knorm^2 (pi/2) sin(pi s_i); 0 = off."""
+        check(self._lib.as_problem_set_bias(self._h, float(b)))
+        return self
+
+    def Set_B(self, b: float):
+        return self.set_bias(b)
+
+    def model(self) -> dict:
+        t, q, b = C.c_int32(), C.c_double(), C.c_double()
+        check(self._lib.as_problem_get_model(self._h, C.byref(t), C.byref(q), C.byref(b)))
+        return dict(tanh=t.value == _abi.AS_MODEL_TANH, q=q.value, b=b.value)
+
     def layout_stats(self, precision: int = AS_PREC_F32_LOGA) -> dict:
         a, b, d = C.c_int32(), C.c_int32(), C.c_int32()
         c = C.c_int64()

@@ -21,6 +21,8 @@ AS_ERR_IO = -5
 AS_PREC_F32_LOGA = 0
 AS_PREC_F64 = 1
 AS_LAYOUT_F32_PAIR = 2  # layout_stats only
+AS_MODEL_CTDS = 0
+AS_MODEL_TANH = 1
 
 _vp = C.c_void_p
 _i32 = C.c_int32
@@ -39,6 +41,9 @@ SIGNATURES = [
     ("as_problem_num_literals", _i32, [_vp]),
     ("as_problem_get_clauses", _i32, [_vp, _pi32, _pi32]),
     ("as_problem_layout_stats", _i32, [_vp, _i32, _pi32, _pi32, C.POINTER(C.c_int64), _pi32]),
+    ("as_problem_set_model", _i32, [_vp, _i32, C.c_double]),
+    ("as_problem_set_bias", _i32, [_vp, C.c_double]),
+    ("as_problem_get_model", _i32, [_vp, _pi32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("as_problem_free", None, [_vp]),
     ("as_rhs_f32", _i32, [_vp, _vp, _vp, _i32, _i32, _vp]),
     ("as_rhs_f64", _i32, [_vp, _vp, _vp, _i32, _vp]),

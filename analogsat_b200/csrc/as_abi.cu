@@ -24,6 +24,9 @@ using namespace asb;
 // layout index of the pair RHS kernel's packing (after the two precisions)
 constexpr int kLayoutPair = AS_LAYOUT_F32_PAIR;
 
+// The plain CTDS right-hand side (CpuSat with b = 0): what every kernel supports.
+bool standard_model(const PackedProblem& q) { return !q.tanh && !(q.b > 0.0); }
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -94,6 +97,9 @@ struct DevicePool {
             DevInstance d;
             d.n = q->n; d.m = q->m; d.k = q->k; d.mp = q->mp; d.nslices = q->nslices;
             d.nslots = q->nslots;
+            d.tanh = q->tanh;
+            d.q = q->q;
+            d.b = q->b;
             d.lit = q->lit.empty() ? nullptr : lit.as<uint32_t>() + ol;
             d.litw = litw.as<uint32_t>() + ow;
             d.slotw = slotw.as<uint32_t>() + ow;
@@ -215,6 +221,9 @@ struct as_problem {
     DevicePool dev[3];        // lazily uploaded for the device primitives
     DevBuf slab[3];           // per-CTA storage of the global-storage primitives
 
+    int tanh = 0;       // CTDS variant (ISat implementation) and its parameters
+    double q = 1.1, b = 0.0;
+
     const PackedProblem& packed(int layout) {
         std::lock_guard<std::mutex> lock(mu_);
         if (!have_[layout]) {
@@ -223,8 +232,12 @@ struct as_problem {
                                                                     : kPackF32Pair);
             have_[layout] = true;
         }
+        packed_[layout].tanh = tanh;
+        packed_[layout].q = q;
+        packed_[layout].b = b;
         return packed_[layout];
     }
+    bool standard_model() const { return !tanh && !(b > 0.0); }
     void pack_all() {}
 };
 
@@ -384,6 +397,32 @@ int32_t as_problem_layout_stats(const as_problem* p, int32_t precision, int32_t*
 
 void as_problem_free(as_problem* p) { delete p; }
 
+int32_t as_problem_set_model(as_problem* p, int32_t model, double q) {
+    if (!p || (model != AS_MODEL_CTDS && model != AS_MODEL_TANH) || !std::isfinite(q))
+        return fail(AS_ERR_BAD_INPUT, "as_problem_set_model: bad argument");
+    std::lock_guard<std::mutex> lock(p->mu_);
+    p->tanh = model == AS_MODEL_TANH ? 1 : 0;
+    p->q = q;
+    for (auto& d : p->dev) d.device = -1;  // re-upload the instance record
+    return AS_OK;
+}
+
+int32_t as_problem_set_bias(as_problem* p, double b) {
+    if (!p || !(b >= 0.0) || !std::isfinite(b)) return fail(AS_ERR_BAD_INPUT, "as_problem_set_bias: need b >= 0");
+    std::lock_guard<std::mutex> lock(p->mu_);
+    p->b = b;
+    for (auto& d : p->dev) d.device = -1;
+    return AS_OK;
+}
+
+int32_t as_problem_get_model(const as_problem* p, int32_t* model, double* q, double* b) {
+    if (!p) return fail(AS_ERR_BAD_INPUT, "null problem");
+    if (model) *model = p->tanh ? AS_MODEL_TANH : AS_MODEL_CTDS;
+    if (q) *q = p->q;
+    if (b) *b = p->b;
+    return AS_OK;
+}
+
 // ---- device primitives ----
 namespace {
 
@@ -433,7 +472,7 @@ template <bool LOGA, int KMAX, bool EXACT>
 int launch_rhs_pair(as_problem* p, const float* x, float* d, int ns, cudaStream_t st, bool* done) {
     constexpr int BT = 1024;
     *done = false;
-    if (reinterpret_cast<uintptr_t>(x) & 3u) return AS_OK;
+    if ((reinterpret_cast<uintptr_t>(x) & 3u) || !p->standard_model()) return AS_OK;
     const auto& q = p->packed(kLayoutPair);
     int dev = 0, sms = 0, optin = 0, occ = 0;
     AS_CUDA(cudaGetDevice(&dev));
@@ -683,10 +722,15 @@ int build_groups(as_solver* s) {
         long gs_units = 0;
         for (int p = 0; p < np; p++)
             if (vs[pv[p]].gs) gs_units += per_problem[p];
+        bool bias = false;  // the bias term's clause-weight sum is reduced per CTA
+        for (const auto& q : s->problems) bias |= q.b > 0.0 || q.tanh;
         int want_cl = 1;
         if (s->forced_cl) want_cl = s->forced_cl;
-        else
+        else if (!bias)
             while (want_cl < 8 && gs_units > 0 && gs_units * want_cl * 2 <= s->sm_count) want_cl *= 2;
+        if (bias && want_cl > 1)
+            return fail(AS_ERR_UNSUPPORTED, "clusters of CTAs per trajectory do not support the bias term "
+                                            "or the tanh variant");
         if (want_cl > 1 && !s->forced_bt) {
             for (int p = 0; p < np; p++) {
                 const Variant& cur = vs[pv[p]];
@@ -866,6 +910,8 @@ constexpr long long kStreamAutoElements = 1ll << 19;  // AS_STORAGE_AUTO: N + M 
 bool use_stream(const as_solver* s) {
     if (s->storage_mode == 3) return true;
     if (s->storage_mode != 0 || s->num_traj <= 0) return false;
+    for (const auto& q : s->problems)
+        if (!standard_model(q)) return false;  // the streamed kernels have the CpuSat RHS only
     for (int t = 0; t < s->num_traj; t++) {
         const auto& q = s->problems[s->traj_problem[t]];
         if ((long long)q.n + q.m < kStreamAutoElements) return false;
@@ -1162,6 +1208,10 @@ int stream_run(as_solver* s) {
 }
 
 int stream_solve(as_solver* s) {
+    for (const auto& q : s->problems)
+        if (!standard_model(q))
+            return fail(AS_ERR_UNSUPPORTED, "the streamed solver has the plain CTDS right-hand side only "
+                                            "(no tanh variant, no bias term)");
     int r = stream_plan(s);
     if (r) return r;
     bool all3 = true, all4 = true;
@@ -1536,6 +1586,9 @@ int32_t as_solver_adjoint(as_solver* s, double t_end, int32_t max_steps, const d
     if (!s || !loss || !grad_x0 || !grad_w) return fail(AS_ERR_BAD_INPUT, "as_solver_adjoint: null argument");
     if (!(t_end > 0.0) || max_steps < 1) return fail(AS_ERR_BAD_INPUT, "as_solver_adjoint: need t_end > 0, max_steps >= 1");
     if (s->num_traj <= 0) return fail(AS_ERR_NO_PROBLEM, "no trajectories set (as_solver_set_states_*)");
+    for (const auto& q : s->problems)
+        if (!standard_model(q))
+            return fail(AS_ERR_UNSUPPORTED, "the adjoint covers the plain CTDS right-hand side only");
     AS_CUDA(cudaSetDevice(s->device));
     const int nt = s->num_traj;
     // one launch shape for all trajectories: the largest instance decides

@@ -34,7 +34,14 @@ struct DevInstance {
     const int32_t* iperm;   // public -> internal variable
     const int32_t* icperm;  // public -> internal clause
     const int32_t* cperm;   // internal -> public clause
+    // CTDS variant (the reference's ISat implementations): tanh = 0 CpuSat / CudaSat,
+    // tanh = 1 CpuSatTanh / CudaSatTanh with slope q; bias b (ISat::Set_B) adds
+    // mean(a) (M/N) b knorm^2 (pi/2) sin(pi s_i) to ds_i (0: off).
+    int tanh;
+    double q, b;
 };
+
+
 
 constexpr float kInvLn2 = 1.4426950408889634f;  // d(log2 a)/dt = (da/dt) / (a ln 2)
 
@@ -50,6 +57,26 @@ template <> struct Arith<float> {
     static __device__ __forceinline__ float add(float a, float b) { return a + b; }
     static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
 };
+
+// The bias term is on: CpuSat adds it when b knorm^2 > 0 (CpuSat.cpp:229), CpuSatTanh
+// always (CpuSatTanh.cpp:233-238, where b = 0 adds zeros).
+__device__ __forceinline__ bool bias_on(const DevInstance& I) { return I.b > 0.0 || I.tanh; }
+
+// mean(a) (M/N) b knorm^2 (pi/2): the per-call factor of the bias term, formed in the
+// reference's expression order from the clause-weight sum (CpuSat.cpp:230-236).
+template <typename T>
+__device__ __forceinline__ T bias_factor(const DevInstance& I, double asum, T knorm) {
+    using A = Arith<T>;
+    const T a = (T)asum / (T)I.m;
+    const T alpha = (T)I.m / (T)I.n;
+    const T bb = A::mul(A::mul((T)I.b, knorm), knorm);
+    return A::mul(A::mul(A::mul(a, alpha), bb), T(1.570796326794897));
+}
+// ... times sin(pi s_i) added to the variable's sum
+__device__ __forceinline__ double bias_term(double f, double s) { return __dmul_rn(f, sin(__dmul_rn(s, 3.141592653589793))); }
+__device__ __forceinline__ float bias_term(float f, float s) { return f * sinf(s * 3.14159265f); }
+__device__ __forceinline__ double tanh_t(double x) { return tanh(x); }
+__device__ __forceinline__ float tanh_t(float x) { return tanhf(x); }
 
 // 2^u with the SFU (relative error ~2^-22, below the FP32 state's own rounding)
 __device__ __forceinline__ float exp2_fast(float u) {
@@ -120,6 +147,45 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
     T dam;
     if constexpr (LOGA) dam = km * km * T(kInvLn2);
     else dam = A::mul(A::mul(am, km), km);
+    if (I.tanh) {
+        // CpuSatTanh: knorm a_m |K_mi| tanh(q (1 - c s_i)) c_mi (KmiFuncTanh,
+        // cpu_helper.h:115-125, leave-one-out product as CpuProdWrapper; k > 10: the
+        // generic CalculateAll, CpuSatTanh.cpp:250-297)
+        const T q = (T)I.q;
+        if (KMAX <= 10 || I.k <= 10) {
+            const T r = A::mul(knorm, am);
+#pragma unroll
+            for (int qq = 0; qq < KMAX; qq++) {
+                if (EXACT || qq < I.k) {
+                    T prod = T(1);
+                    bool first = true;
+#pragma unroll
+                    for (int l = 0; l < KMAX; l++) {
+                        if (l != qq && (EXACT || l < I.k)) {
+                            prod = first ? f[l] : A::mul(prod, f[l]);
+                            first = false;
+                        }
+                    }
+                    const T rr = A::mul(A::mul(r, fabs(prod)), tanh_t(A::mul(q, f[qq])));
+                    cs[w[qq].slot()] = w[qq].neg() ? -rr : rr;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int qq = 0; qq < KMAX; qq++) {
+                if (EXACT || qq < I.k) {
+                    T temp = T(1);
+#pragma unroll
+                    for (int l = 0; l < KMAX; l++)
+                        if (EXACT || l < I.k) temp = A::mul(temp, l == qq ? T(1) : f[l]);
+                    T rr = A::mul(A::mul(knorm, am), fabs(temp));
+                    rr = w[qq].neg() ? -rr : rr;
+                    cs[w[qq].slot()] = A::mul(rr, tanh_t(A::mul(q, f[qq])));
+                }
+            }
+        }
+        return dam;
+    }
     if (KMAX <= 10 || I.k <= 10) {
         const T r = A::mul(A::mul(km, knorm), am);
 #pragma unroll

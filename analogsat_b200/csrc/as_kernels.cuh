@@ -166,11 +166,14 @@ struct Solver {
     // One RHS evaluation at stage S.  The stage input is formed on the fly from the
     // stage vectors; the derivative lands in K_S, or for S == 6 is consumed at once
     // into xnew (stored in K2, dead after the stage-6 input) and the error norm.
+    // red_b: one slot per warp for the clause-weight sum of the bias term (CL == 1).
     template <int S>
     static __device__ __forceinline__ void eval(const Grp<CL>& g, const DevInstance& I, T* sy, T* cs, T knorm,
-                                                const Stages<T>& st, T hT, T h0T, ET& errmax) {
+                                                const Stages<T>& st, T hT, T h0T, ET& errmax, double* red_b) {
         const int tid = g.gtid, nt = g.gnt;
         const int n = I.n;
+        const bool bias = bias_on(I);
+        double asum = 0.0;
         for (int v = tid; v < n; v += nt)
             sy[v] = stage_in<S>(st.X[v], st.K1[v], st.K2[v], st.K3[v], st.K4[v], st.K5[v], hT);
         g.sync();
@@ -182,6 +185,7 @@ struct Solver {
             if constexpr (LOGA) am = exp2_fast(y);
             else am = y;
             const T d = clause_phase<T, LOGA, KMAX, EXACT, ENC>(I, m, sy, cs, am, knorm);
+            if (bias) asum += (double)am;
             if constexpr (S == 1) st.K1[e] = d;
             if constexpr (S == 2) st.K2[e] = d;
             if constexpr (S == 3) st.K3[e] = d;
@@ -193,9 +197,21 @@ struct Solver {
                 st.K2[e] = rk_new<T>(x, k1, k3, k4, d, hT);
             }
         }
+        T bf = T(0);
+        if (bias) {  // per-warp partial sums, read back by every thread after the barrier
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) asum += __shfl_xor_sync(0xffffffffu, asum, o);
+            if ((threadIdx.x & 31) == 0) red_b[threadIdx.x >> 5] = asum;
+        }
         g.sync();
+        if (bias) {
+            double tot = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += red_b[w];
+            bf = bias_factor<T>(I, tot, knorm);
+        }
         for (int v = tid; v < n; v += nt) {
-            const T d = var_phase<T>(I, v, cs);
+            T d = var_phase<T>(I, v, cs);
+            if (bias) d = Arith<T>::add(d, bias_term(bf, sy[v]));
             if constexpr (S == 1) st.K1[v] = d;
             if constexpr (S == 2) st.K2[v] = d;
             if constexpr (S == 3) st.K3[v] = d;
@@ -227,6 +243,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
     using S = Solver<T, LOGA, KMAX, EXACT, ENC, CL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red_d[36];
+    __shared__ double red_b[32];
     __shared__ int red_i[33];
     __shared__ int s_unit, s_flag;
     const Grp<CL> g;
@@ -273,7 +290,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
             for (int b = 0; b < P.batch; b++) {
                 // ---- CpuRungeKutta::Step, count = 1 ----
                 T dummy = T(0);
-                S::template eval<1>(g, I, sy, cs, knorm, st, T(0), T(0), dummy);
+                S::template eval<1>(g, I, sy, cs, knorm, st, T(0), T(0), dummy, red_b);
                 rhs++;
                 const double h0 = hnext;
                 const T h0T = (T)h0;
@@ -281,11 +298,11 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
                 while (true) {
                     const T hT = (T)h;
                     T em = T(0);
-                    S::template eval<2>(g, I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<3>(g, I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<4>(g, I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<5>(g, I, sy, cs, knorm, st, hT, h0T, em);
-                    S::template eval<6>(g, I, sy, cs, knorm, st, hT, h0T, em);
+                    S::template eval<2>(g, I, sy, cs, knorm, st, hT, h0T, em, red_b);
+                    S::template eval<3>(g, I, sy, cs, knorm, st, hT, h0T, em, red_b);
+                    S::template eval<4>(g, I, sy, cs, knorm, st, hT, h0T, em, red_b);
+                    S::template eval<5>(g, I, sy, cs, knorm, st, hT, h0T, em, red_b);
+                    S::template eval<6>(g, I, sy, cs, knorm, st, hT, h0T, em, red_b);
                     rhs += 5;
                     attempts++;
                     // step-size control (CpuRungeKutta.cpp:229-259): one thread evaluates
@@ -398,6 +415,7 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
                                                         long long slab_stride) {
     constexpr int ENC = GS ? 1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red_b[BT / 32];
     T* sy = GS ? slab + (long long)blockIdx.x * slab_stride : reinterpret_cast<T*>(smem_raw);
     T* ab = sy + ((I.n + 1 + 3) & ~3);  // clause weights in internal clause order
     T* cs = ab + ((I.m + 3) & ~3);
@@ -413,16 +431,35 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
         for (int j = tid; j < I.m; j += BT) ab[__ldg(I.icperm + j)] = X[n + j];
         if (tid == 0) sy[n] = T(-1);
         __syncthreads();
+        const bool bias = bias_on(I);
+        double asum = 0.0;
         for (int m = tid; m < I.m; m += BT) {
             const T a = ab[m];
             T am;
             if constexpr (LOGA) am = exp2_fast(a);
             else am = a;
             ab[m] = clause_phase<T, LOGA, KMAX, EXACT, ENC>(I, m, sy, cs, am, knorm);
+            if (bias) asum += (double)am;
+        }
+        if (bias) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) asum += __shfl_xor_sync(0xffffffffu, asum, o);
+            if ((tid & 31) == 0) red_b[tid >> 5] = asum;
         }
         __syncthreads();
-        // ds in internal order -> sy (no longer read) -> public order, coalesced
-        for (int v = tid; v < n; v += BT) sy[v] = var_phase<T>(I, v, cs);
+        T bf = T(0);
+        if (bias) {
+            double tot = 0.0;
+            for (int w = 0; w < BT / 32; w++) tot += red_b[w];
+            bf = bias_factor<T>(I, tot, knorm);
+        }
+        // ds in internal order -> sy (no longer read) -> public order, coalesced; the
+        // bias term reads the stage spin of its own element before overwriting it
+        for (int v = tid; v < n; v += BT) {
+            T d = var_phase<T>(I, v, cs);
+            if (bias) d = Arith<T>::add(d, bias_term(bf, sy[v]));
+            sy[v] = d;
+        }
         __syncthreads();
         for (int i = tid; i < n; i += BT) D[i] = sy[__ldg(I.iperm + i)];
         for (int j = tid; j < I.m; j += BT) D[n + j] = ab[__ldg(I.icperm + j)];

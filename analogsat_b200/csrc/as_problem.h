@@ -81,6 +81,10 @@ struct PackedProblem {
     std::vector<int32_t> icperm;   // public -> internal clause
     int max_degree = 0;
     long bank_wavefronts = 0;      // shared-memory wavefronts of one gather pass (>= 32-clause groups x k)
+    // CTDS variant of the instance (ISat implementation and parameters): tanh = 1 is
+    // CpuSatTanh with slope q, b the bias coefficient (ISat::Set_B; 0 = off).
+    int tanh = 0;
+    double q = 1.1, b = 0.0;
 };
 
 enum PackMode : int {

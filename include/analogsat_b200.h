@@ -98,6 +98,21 @@ int32_t as_problem_layout_stats(const as_problem* p, int32_t precision, int32_t*
 
 void as_problem_free(as_problem* p);
 
+/* CTDS variant of a problem, the reference's choice of ISat class: AS_MODEL_CTDS is
+ * CpuSat / CudaSat1-3, AS_MODEL_TANH is CpuSatTanh / CudaSatTanh1-3 with slope q
+ * (AnalogSAT/cpu_sat/CpuSatTanh.h:35, Set_Q at :92; default q = 1.1,
+ * CpuSatTanh.cpp:40): ds_i = sum_m knorm a_m |K_mi| tanh(q (1 - c_mi s_i)) c_mi.
+ * Device RHS (as_rhs_*) and solvers created afterwards use it.  The streamed
+ * solver, thread-block clusters and the adjoint support AS_MODEL_CTDS with b = 0
+ * only (AS_ERR_UNSUPPORTED otherwise). */
+#define AS_MODEL_CTDS 0
+#define AS_MODEL_TANH 1
+int32_t as_problem_set_model(as_problem* p, int32_t model, double q);
+/* ISat::Set_B (AnalogSAT/solver/ISat.h:53; applied in CpuSat.cpp:229-238): adds
+ * mean(a) (M/N) b knorm^2 (pi/2) sin(pi s_i) to ds_i; b >= 0, 0 = off (default). */
+int32_t as_problem_set_bias(as_problem* p, double b);
+int32_t as_problem_get_model(const as_problem* p, int32_t* model, double* q, double* b);
+
 /* ---- device primitives (ISat, AnalogSAT/solver/ISat.h:31-87) -------------- */
 
 /* ISat::GetDerivatives over `num_states` states at once (CpuSat.cpp:65-94,

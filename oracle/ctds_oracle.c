@@ -18,7 +18,16 @@ struct orc_problem {
     int* C;      /* clause-major [m][k], signed 1-based literals, 0 = padding
                     (AnalogSAT/cpu_sat/CpuSat.cpp:353-377, GetC at 385-388) */
     double knorm; /* 2^-k with k the MAX clause length (CpuSat.cpp:355) */
+    int tanh;     /* CpuSatTanh instead of CpuSat (AnalogSAT/cpu_sat/CpuSatTanh.cpp) */
+    double q;     /* its slope (CpuSatTanh.cpp:40 default 1.1) */
+    double b;     /* bias coefficient, ISat::Set_B (0 = off) */
 };
+
+void orc_problem_set_model(orc_problem* p, int tanh_model, double q, double b) {
+    p->tanh = tanh_model;
+    p->q = q;
+    p->b = b;
+}
 
 /* SatProblem::AddClauses (AnalogSAT/problem/SatProblem.cpp:64-95): zero literals are
  * filtered, empty clauses dropped, N = max |literal|, K = max clause length. */
@@ -49,6 +58,7 @@ orc_problem* orc_problem_new(const int* lits, const int* lens, int m_in) {
         total += lens[j];
     }
     p->knorm = pow(2.0, -(double)p->k);
+    p->q = 1.1;
     return p;
 }
 
@@ -72,6 +82,7 @@ static void rhs_internal(const orc_problem* p, const double* x, double* rhs, int
     double f[64];
     int idx[64];
     int j, q, l;
+    double sum = 0.0;
     memset(rhs, 0, sizeof(double) * (size_t)(n + m + 1));
     for (j = 0; j < m; j++) {
         double km = knorm, am, r;
@@ -88,6 +99,33 @@ static void rhs_internal(const orc_problem* p, const double* x, double* rhs, int
         } else {
             am = x[n + 1 + j];
             rhs[n + 1 + j] = am * km * km;
+        }
+        sum += am;
+        if (p->tanh) {
+            /* CpuSatTanh::CalculateAllEx<K> / KmiFuncTanh (CpuSatTanh.cpp:203-244,
+             * cpu_helper.h:115-125) for K <= 10, CalculateAll (CpuSatTanh.cpp:250-297) */
+            if (k <= 10) {
+                r = knorm * am;
+                for (q = 0; q < k; q++) {
+                    double prod = 1.0, rr;
+                    int first = 1;
+                    if (idx[q] == 0) break;
+                    for (l = 0; l < k; l++) {
+                        if (l == q) continue;
+                        if (first) { prod = f[l]; first = 0; } else prod = prod * f[l];
+                    }
+                    rr = r * (prod < 0 ? -prod : prod) * tanh(p->q * f[q]);
+                    rr *= idx[q] < 0 ? -1.0 : 1.0;
+                    rhs[abs(idx[q])] += rr;
+                }
+            } else {
+                for (q = 0; q < k; q++) {
+                    double temp = 1.0, sign = idx[q] < 0 ? -1.0 : 1.0;
+                    for (l = 0; l < k; l++) temp *= (l == q) ? 1.0 : f[l];
+                    rhs[abs(idx[q])] += knorm * am * fabs(temp) * sign * tanh(p->q * f[q]);
+                }
+            }
+            continue;
         }
         if (k <= 10) {
             r = km * knorm * am;
@@ -109,6 +147,17 @@ static void rhs_internal(const orc_problem* p, const double* x, double* rhs, int
                 for (l = 0; l < k; l++) temp *= (l == q) ? 1.0 : f[l];
                 rhs[abs(idx[q])] += 2.0 * temp * knorm * am * sign;
             }
+        }
+    }
+    {
+        /* the bias term (CpuSat.cpp:228-238: only when b knorm^2 > 0; CpuSatTanh.cpp:
+         * 233-238 and 298-302: always) */
+        const double bb = p->b * knorm * knorm;
+        if (bb > 0.0 || p->tanh) {
+            const double a = sum / m, alpha = (double)m / (double)n;
+            int i;
+            for (i = 1; i < n + 1; i++)
+                rhs[i] += a * alpha * bb * 1.570796326794897 * sin(x[i] * 3.141592653589793);
         }
     }
     rhs[0] = 0.0;

@@ -22,6 +22,9 @@ typedef struct orc_problem orc_problem;
 /* SatProblem::AddClauses semantics (AnalogSAT/problem/SatProblem.cpp:64-95). */
 orc_problem* orc_problem_new(const int* lits, const int* lens, int m);
 void orc_problem_free(orc_problem* p);
+/* CTDS variant: tanh_model = 1 restates CpuSatTanh (slope q), b the bias coefficient
+ * (ISat::Set_B); default CpuSat with b = 0. */
+void orc_problem_set_model(orc_problem* p, int tanh_model, double q, double b);
 void orc_problem_info(const orc_problem* p, int* n, int* m, int* k);
 
 /* CpuSat::GetDerivatives (AnalogSAT/cpu_sat/CpuSat.cpp:65-94, 199-241). */

@@ -74,6 +74,8 @@ class Oracle:
         L.orc_fixed_loss.argtypes = [C.c_void_p, _f64p, C.c_void_p, _f64p, C.c_int, C.c_void_p]
         L.orc_adjoint.restype = C.c_double
         L.orc_adjoint.argtypes = [C.c_void_p, _f64p, C.c_void_p, _f64p, C.c_int, _f64p, _f64p]
+        L.orc_problem_set_model.restype = None
+        L.orc_problem_set_model.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
         self.L = L
 
     class Problem:
@@ -93,6 +95,10 @@ class Oracle:
 
     def problem(self, lits, lens):
         return Oracle.Problem(self.L, lits, lens)
+
+    def set_model(self, p, tanh=False, q=1.1, b=0.0):
+        """CTDS variant of problem p: tanh restates CpuSatTanh (slope q); b the bias."""
+        self.L.orc_problem_set_model(p.h, int(tanh), float(q), float(b))
 
     def problem_from_clauses(self, clauses):
         return self.problem(*_flat(clauses))
@@ -212,7 +218,13 @@ class Reference:
                                        C.POINTER(C.c_double)]
         L.ref_minisat.restype = C.c_int
         L.ref_minisat.argtypes = [C.c_void_p, C.c_void_p]
+        L.ref_set_model.restype = None
+        L.ref_set_model.argtypes = [C.c_int, C.c_double, C.c_double]
         self.L = L
+
+    def set_model(self, tanh=False, q=1.1, b=0.0):
+        """CTDS variant of every following call: CpuSatTanh (slope q) or CpuSat, Set_B(b)."""
+        self.L.ref_set_model(int(tanh), float(q), float(b))
 
     class Problem:
         def __init__(self, L, h, planted=None):

@@ -29,6 +29,7 @@
 #include "../io/CnfReader.h"
 #include "../io/CnfWriter.h"
 #include "../cpu_sat/CpuSat.h"
+#include "../cpu_sat/CpuSatTanh.h"
 #include "../cpu_sat/CpuRungeKutta.h"
 #include "../solver/SatSolver.h"
 #include "minisat.h"
@@ -53,12 +54,33 @@ struct MemCnf : public Minisat::MemoryCNF {
     int NextInt() override { return content[pos++]; }
 };
 
+// CTDS variant used by every entry point below (set by ref_set_model): CpuSat or
+// CpuSatTanh (with Set_Q), and ISat::Set_B.
+struct Model {
+    int tanh = 0;
+    double q = 1.1, b = 0.0;
+};
+Model g_model;
+
+template <typename T>
+ISat<T, CpuODEState<T>>* make_sat() {
+    if (g_model.tanh) {
+        CpuSatTanh<T>* s = new CpuSatTanh<T>();
+        s->Set_Q((T)g_model.q);
+        s->Set_B((T)g_model.b);
+        return s;
+    }
+    CpuSat<T>* s = new CpuSat<T>();
+    s->Set_B((T)g_model.b);
+    return s;
+}
+
 template <typename T>
 struct RefSolver {
     CpuSatSolver<T> solver;
     CpuRungeKutta<T>* rk;
     RefSolver(const SatProblem& p, T eps)
-        : solver(new CpuSat<T>(), rk = new CpuRungeKutta<T>()) {
+        : solver(make_sat<T>(), rk = new CpuRungeKutta<T>()) {
         rk->SetEpsilon(eps);
         solver.SetProblem(p);
     }
@@ -68,14 +90,14 @@ template <typename T>
 int rhs_impl(void* handle, const T* state_pub, T* dxdt_pub) {
     try {
         const SatProblem& p = *static_cast<SatProblem*>(handle);
-        CpuSat<T> sat;
-        sat.SetProblem(p);
-        std::unique_ptr<ISatState<T, CpuODEState<T>>> x(sat.MakeState());
-        std::unique_ptr<ISatState<T, CpuODEState<T>>> d(sat.MakeState());
+        std::unique_ptr<ISat<T, CpuODEState<T>>> sat(make_sat<T>());
+        sat->SetProblem(p);
+        std::unique_ptr<ISatState<T, CpuODEState<T>>> x(sat->MakeState());
+        std::unique_ptr<ISatState<T, CpuODEState<T>>> d(sat->MakeState());
         const int nm = p.Get_N() + p.Get_M();
         std::vector<T> v(state_pub, state_pub + nm);
         x->CopyFrom(v);
-        sat.GetDerivatives(*d, *x, (T)0);
+        sat->GetDerivatives(*d, *x, (T)0);
         std::vector<T> out;
         d->CopyTo(out);
         std::memcpy(dxdt_pub, out.data(), sizeof(T) * nm);
@@ -105,7 +127,7 @@ int steps_impl(void* handle, const T* ic, T eps, int nsteps, double* times, doub
     try {
         const SatProblem& p = *static_cast<SatProblem*>(handle);
         const int nm = p.Get_N() + p.Get_M();
-        auto sat = std::make_shared<CpuSat<T>>();
+        std::shared_ptr<ISat<T, CpuODEState<T>>> sat(make_sat<T>());
         sat->SetProblem(p);
         CpuRungeKutta<T> rk;
         rk.SetEpsilon(eps);
@@ -233,6 +255,14 @@ void* refp_read_cnf(const char* path, char* msg, int msglen) {
 }
 
 void refp_free(void* h) { delete static_cast<SatProblem*>(h); }
+
+// CTDS variant of the following calls: tanh = 1 builds CpuSatTanh (slope q) instead
+// of CpuSat; b is passed to ISat::Set_B.  Not thread-safe against running solves.
+void ref_set_model(int tanh, double q, double b) {
+    g_model.tanh = tanh;
+    g_model.q = q;
+    g_model.b = b;
+}
 
 int ref_rhs_d(void* h, const double* x, double* d) { return rhs_impl<double>(h, x, d); }
 int ref_rhs_f(void* h, const float* x, float* d) { return rhs_impl<float>(h, x, d); }

@@ -24,3 +24,11 @@ def golden():
     import numpy as np
     path = os.path.join(ROOT, "tests", "golden", "golden.npz")
     return dict(np.load(path, allow_pickle=False))
+
+
+@pytest.fixture(scope="session")
+def golden_models():
+    """The reference's CTDS variants (CpuSatTanh, bias term) on golden.npz's problems."""
+    import numpy as np
+    path = os.path.join(ROOT, "tests", "golden", "golden_models.npz")
+    return dict(np.load(path, allow_pickle=False))

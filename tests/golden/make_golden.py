@@ -3,6 +3,7 @@ CPU solver and MiniSat, compiled from the reference's own sources into
 oracle/_ref/libanalogsat_ref.so (oracle/Makefile).
 
 Run in a container that has the reference tree:  python tests/golden/make_golden.py
+(and `--models` for golden_models.npz, the tanh and bias variants).
 Every array below is an output of the reference code itself (its makers, CpuSat,
 CpuRungeKutta, SatSolver, CnfWriter and MiniSat), so the committed fixtures pin both
 our C restatement (oracle/ctds_oracle.c) and the CUDA path to the reference.
@@ -129,5 +130,35 @@ def main():
     print("wrote", len(out), "arrays")
 
 
+MODELS = {"tanh": (1, 1.1, 0.0), "tanh_q2_b3": (1, 2.0, 3.0), "bias20": (0, 1.1, 20.0)}
+
+
+def models():
+    """tests/golden/golden_models.npz: the reference's CTDS variants -- CpuSatTanh
+    (Set_Q) and the bias term (ISat::Set_B) -- on the problems and states of
+    golden.npz: FP64 RHS vectors and 30 single steps of CpuRungeKutta<double>."""
+    build()
+    R = Reference()
+    g = np.load(os.path.join(HERE, "golden.npz"))
+    out = {}
+    for tag in ("p50", "mix", "k12", "r4", "p200"):
+        p = R.problem(g[f"{tag}/literals"], g[f"{tag}/lengths"])
+        for name, (tanh, q, b) in MODELS.items():
+            R.set_model(tanh, q, b)
+            out[f"{tag}/{name}/rhs_f64"] = np.stack([R.rhs(p, x) for x in g[f"{tag}/rhs_states"]])
+            if f"{tag}/traj_ic" in g.files:
+                tr = R.steps(p, g[f"{tag}/traj_ic"], 1e-6, 30)
+                out[f"{tag}/{name}/traj_time"] = tr["time"]
+                out[f"{tag}/{name}/traj_h"] = tr["h"]
+                out[f"{tag}/{name}/traj_rhs"] = tr["rhs"]
+                out[f"{tag}/{name}/traj_final"] = tr["states"][-1]
+        R.set_model()
+    np.savez_compressed(os.path.join(HERE, "golden_models.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
 if __name__ == "__main__":
-    main()
+    if "--models" in sys.argv:
+        models()
+    else:
+        main()

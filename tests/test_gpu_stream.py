@@ -1,4 +1,4 @@
-"""The streamed solver (storage mode 3): four trajectories per lane group, state
+"""The streamed solver (storage mode 3): eight trajectories per lane group, state
 interleaved in device memory, one RK attempt per pass of per-stage kernels.
 
 Checks: in FP64 (explicitly rounded arithmetic) every lane follows exactly the

@@ -150,3 +150,24 @@ def test_oracle_adjoint_matches_central_differences(oracle):
         fd = (oracle.fixed_loss(p, x0, hs, w + eh * dw) - oracle.fixed_loss(p, x0, hs, w - eh * dw)) / (2 * eh)
         errs.append(abs(fd - gw @ dw) / max(abs(fd), 1e-12))
     assert np.median(errs) < 1e-7 and max(errs) < 1e-4
+
+
+MODELS = {"tanh": (True, 1.1, 0.0), "tanh_q2_b3": (True, 2.0, 3.0), "bias20": (False, 1.1, 20.0)}
+
+
+@pytest.mark.parametrize("name", list(MODELS))
+@pytest.mark.parametrize("tag", ["p50", "mix", "k12", "r4", "p200"])
+def test_model_variants_bit_exact(oracle, golden, golden_models, tag, name):
+    """CpuSatTanh (Set_Q) and the bias term (Set_B): the C restatement reproduces the
+    reference's RHS vectors and 30 Cash-Karp steps bit for bit."""
+    tanh, q, b = MODELS[name]
+    p = _problem(oracle, golden, tag)
+    oracle.set_model(p, tanh, q, b)
+    for x, ref in zip(golden[f"{tag}/rhs_states"], golden_models[f"{tag}/{name}/rhs_f64"]):
+        d = oracle.rhs(p, x)
+        assert np.array_equal(d, ref), np.abs(d - ref).max()
+    if f"{tag}/{name}/traj_time" in golden_models:
+        tr = oracle.steps(p, golden[f"{tag}/traj_ic"], 1e-6, 30)
+        assert np.array_equal(tr["time"], golden_models[f"{tag}/{name}/traj_time"])
+        assert np.array_equal(tr["rhs"], golden_models[f"{tag}/{name}/traj_rhs"])
+        assert np.array_equal(tr["states"][-1], golden_models[f"{tag}/{name}/traj_final"])
