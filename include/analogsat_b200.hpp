@@ -120,6 +120,20 @@ public:
     int Get_M() const { return nmk(1); }
     int Get_K() const { return nmk(2); }
 
+    // The CTDS variant, which the reference chooses by class (CpuSat / CpuSatTanh with
+    // Set_Q, AnalogSAT/cpu_sat/CpuSatTanh.h:92) and ISat::Set_B (AnalogSAT/solver/
+    // ISat.h:50-53).  Solvers take the variant when SetProblem is called.
+    void SetTanh(bool on, double q = 1.1) {
+        tanh_ = on;
+        q_ = q;
+        if (h_) apply_model();
+    }
+    void Set_B(double b) {
+        b_ = b;
+        if (h_) apply_model();
+    }
+    double Get_B() const { return b_; }
+
     // SatProblem::GetAllClauses (SatProblem.cpp:104-110)
     void GetAllClauses(std::vector<int>& literals, std::vector<int>& lengths) const {
         const int32_t nl = as_problem_num_literals(handle());
@@ -136,11 +150,18 @@ public:
 private:
     std::vector<int32_t> lits_, lens_;
     std::shared_ptr<as_problem> h_;
+    bool tanh_ = false;
+    double q_ = 1.1, b_ = 0.0;
 
     void rebuild() {
         as_problem* h = nullptr;
         check(as_problem_create(lits_.data(), lens_.data(), (int32_t)lens_.size(), &h));
         h_.reset(h, as_problem_free);
+        apply_model();
+    }
+    void apply_model() {
+        check(as_problem_set_model(h_.get(), tanh_ ? AS_MODEL_TANH : AS_MODEL_CTDS, q_));
+        check(as_problem_set_bias(h_.get(), b_));
     }
     int nmk(int i) const {
         int32_t v[3];
