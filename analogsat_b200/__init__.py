@@ -16,6 +16,7 @@ exceptions' counterpart.  Every call goes to the CUDA library; there is no CPU p
 from __future__ import annotations
 
 import ctypes as C
+import os
 from enum import IntEnum
 
 import numpy as np
@@ -336,6 +337,15 @@ class SatSolver:
               else self._lib.as_solver_get_states_f64)
         check(fn(self._h, out.ctypes.data_as(C.c_void_p)))
         return out
+
+    def WriteResult(self, traj: int, path: str):
+        """The reference frontend's MiniSat-compatible result file (SAT / INDET + assignment)."""
+        check(self._lib.as_solver_write_result(self._h, int(traj), os.fsencode(path)))
+
+    def AppendPerf(self, traj: int, path: str, sample: str, solver_name: str = "analogsat_b200"):
+        """Appends the reference bench's tab-separated perf line for one trajectory."""
+        check(self._lib.as_solver_append_perf(self._h, int(traj), os.fsencode(path), sample.encode(),
+                                              solver_name.encode()))
 
     def GetSatState(self, traj: int = 0, dtype=np.float64) -> np.ndarray:
         allst = self.GetSatStates(dtype)

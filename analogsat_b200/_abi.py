@@ -42,6 +42,9 @@ SIGNATURES = [
     ("as_problem_get_clauses", _i32, [_vp, _pi32, _pi32]),
     ("as_problem_layout_stats", _i32, [_vp, _i32, _pi32, _pi32, C.POINTER(C.c_int64), _pi32]),
     ("as_problem_set_model", _i32, [_vp, _i32, C.c_double]),
+    ("as_result_message", C.c_char_p, [_i32]),
+    ("as_solver_write_result", _i32, [_vp, _i32, C.c_char_p]),
+    ("as_solver_append_perf", _i32, [_vp, _i32, C.c_char_p, C.c_char_p, C.c_char_p]),
     ("as_problem_set_bias", _i32, [_vp, C.c_double]),
     ("as_problem_get_model", _i32, [_vp, _pi32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("as_problem_free", None, [_vp]),

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <ctime>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -269,6 +271,7 @@ struct as_solver {
     int batch = 20;
     double eps = 1e-4;
     double wall_budget = 0.0;
+    double last_wall = 0.0, last_cpu = 0.0;  // host wall / CPU seconds of the last as_solver_solve
     int stop_on_first = 0;
     int track_best = 0;
     int forced_bt = 0;
@@ -1293,9 +1296,66 @@ int32_t as_solver_sync(as_solver* s) {
 }
 
 int32_t as_solver_solve(as_solver* s) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    const auto w0 = std::chrono::steady_clock::now();
+    const std::clock_t c0 = std::clock();
     int r = as_solver_solve_async(s, nullptr);
+    if (!r) r = as_solver_sync(s);
+    s->last_wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+    s->last_cpu = (double)(std::clock() - c0) / CLOCKS_PER_SEC;
+    return r;
+}
+
+const char* as_result_message(int32_t result) {
+    switch (result) {  // GetSatResultMessage (AnalogSAT/solver/SatResult.cpp)
+        case SAT_SOLUTION_FOUND: return "solution found";
+        case SAT_UNDERFLOW: return "underflow";
+        case SAT_ODE_INTERRUPTED: return "user interrupt";
+        case SAT_MAXTIME_REACHED: return "maximum time reached";
+        case SAT_MAXITER_REACHED: return "maximum steps reached";
+        default: return "unknown result";
+    }
+}
+
+int32_t as_solver_write_result(as_solver* s, int32_t traj, const char* path) {
+    if (!s || !path) return fail(AS_ERR_BAD_INPUT, "as_solver_write_result: null argument");
+    if (traj < 0 || traj >= s->num_traj) return fail(AS_ERR_BAD_INPUT, "trajectory index out of range");
+    std::vector<int32_t> status(s->num_traj);
+    int r = as_solver_get_results(s, status.data(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     if (r) return r;
-    return as_solver_sync(s);
+    const int n = s->problems[s->traj_problem[traj]].n;
+    std::vector<double> x((size_t)s->total_values);
+    r = as_solver_get_states_f64(s, x.data());
+    if (r) return r;
+    const double* st = x.data() + s->traj_off[traj];
+    FILE* f = std::fopen(path, "w");
+    if (!f) return fail(AS_ERR_IO, std::string("cannot open result file to write: ") + path);
+    // MiniSat-compatible: SAT or INDET (an incomplete solver cannot prove UNSAT), then
+    // the assignment as signed variable numbers terminated by 0 (cnf_runner.cpp:280-304)
+    std::fprintf(f, "%s\n", status[traj] == SAT_SOLUTION_FOUND ? "SAT" : "INDET");
+    if (n > 0) std::fprintf(f, "%d", st[0] > 0 ? 1 : -1);
+    for (int i = 1; i < n; i++) std::fprintf(f, " %d", st[i] > 0.0 ? i + 1 : -i - 1);
+    std::fprintf(f, " 0\n");
+    const bool ok = std::fclose(f) == 0;
+    return ok ? AS_OK : fail(AS_ERR_IO, std::string("cannot write ") + path);
+}
+
+int32_t as_solver_append_perf(as_solver* s, int32_t traj, const char* path, const char* sample,
+                              const char* solver_name) {
+    if (!s || !path || !sample || !solver_name) return fail(AS_ERR_BAD_INPUT, "as_solver_append_perf: null argument");
+    if (traj < 0 || traj >= s->num_traj) return fail(AS_ERR_BAD_INPUT, "trajectory index out of range");
+    std::vector<int32_t> status(s->num_traj), rhs(s->num_traj);
+    int r = as_solver_get_results(s, status.data(), nullptr, nullptr, rhs.data(), nullptr, nullptr, nullptr, nullptr);
+    if (r) return r;
+    cudaDeviceProp prop;
+    AS_CUDA(cudaGetDeviceProperties(&prop, s->device));
+    FILE* f = std::fopen(path, "a");
+    if (!f) return fail(AS_ERR_IO, std::string("cannot open ") + path);
+    // sample, GPU, solver, answer, wall time, CPU time, RHS count (bench_runner.cpp:331-343)
+    std::fprintf(f, "%s\t%s\t%s\t%s\t%lf\t%lf\t%d\n", sample, prop.name, solver_name,
+                 as_result_message(status[traj]), s->last_wall, s->last_cpu, rhs[traj]);
+    const bool ok = std::fclose(f) == 0;
+    return ok ? AS_OK : fail(AS_ERR_IO, std::string("cannot write ") + path);
 }
 
 int32_t as_solver_get_results(as_solver* s, int32_t* status, double* time, int32_t* steps, int32_t* rhs,

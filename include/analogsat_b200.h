@@ -200,6 +200,19 @@ const void* as_solver_states_device(as_solver* s);
  * solve): bits[w] bit b = variable 32w+b+1 TRUE.  bits holds ceil(N/32) words. */
 int32_t as_solver_get_best_assignment(as_solver* s, int32_t traj, uint32_t* bits);
 
+/* GetSatResultMessage (AnalogSAT/solver/SatResult.cpp:23-34) for a SatResult code. */
+const char* as_result_message(int32_t result);
+/* The reference frontend's result file for one trajectory (Frontend/src/cnf_runner.cpp:
+ * 280-304): "SAT" or "INDET", then the final assignment as signed variable numbers
+ * ending in 0, MiniSat-compatible.  Overwrites path. */
+int32_t as_solver_write_result(as_solver* s, int32_t traj, const char* path);
+/* Appends the reference bench's perf line for one trajectory (Frontend/src/
+ * bench_runner.cpp:331-343): sample, GPU name, solver name, result message, wall and
+ * CPU seconds of the last as_solver_solve call (the whole batched call), RHS count;
+ * tab-separated. */
+int32_t as_solver_append_perf(as_solver* s, int32_t traj, const char* path, const char* sample,
+                              const char* solver_name);
+
 /* Launch shape of the last solve's final launch group: threads per CTA, CTAs
  * launched, dynamic shared memory per CTA and resident CTAs per SM. */
 int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas, int32_t* smem_bytes,

@@ -142,3 +142,13 @@ def test_packing_layout_quality():
     assert sp["bank_wavefronts"] <= 1.4 * k * ((m + 15) // 16)
     big = SatProblem.from_arrays(*make_instance("fast", 40000, 200000, 4, seed=1)[:2])
     assert not big.layout_stats()["compact"]
+
+
+def test_result_messages():
+    """GetSatResultMessage's strings (AnalogSAT/solver/SatResult.cpp)."""
+    from analogsat_b200 import load
+    lib = load()
+    msgs = {0: b"solution found", 1: b"underflow", 2: b"user interrupt", 3: b"maximum time reached",
+            4: b"maximum steps reached", 5: b"unknown result", 99: b"unknown result"}
+    for code, msg in msgs.items():
+        assert lib.as_result_message(code) == msg

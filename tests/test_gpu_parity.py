@@ -320,3 +320,40 @@ def test_maxsat_best_assignment():
         sat = np.where(c > 0, best[v], ~best[v]).any(axis=1)
         assert (~sat).sum() == r["min_violations"][t]
         assert r["min_violations"][t] <= r["violations"][t]
+
+
+def test_result_file_and_perf_line(golden, tmp_path):
+    """The reference frontend's output formats: the MiniSat-compatible result file of a
+    solved trajectory (its assignment satisfies the formula) and an unsolved one
+    (INDET), and the tab-separated perf line."""
+    from analogsat_b200 import SatSolver
+    from analogsat_b200.instances import is_satisfied
+    p = _prob(golden, "p50")
+    s = SatSolver([p], precision=1)
+    s.SetEpsilon(1e-6); s.SetBatchSize(50); s.SetMaxSteps(200000); s.SetMaxTime(1e8)
+    ics = golden["p50/solve_ics"][:2].copy()
+    s.SetSatStates([0, 0], ics)
+    s.Solve()
+    r = s.results()
+    assert r["status"][0] == 0
+    out = tmp_path / "p50.out"
+    s.WriteResult(0, str(out))
+    head, body = out.read_text().splitlines()
+    assert head == "SAT"
+    lits = [int(t) for t in body.split()]
+    assert lits[-1] == 0 and [abs(v) for v in lits[:-1]] == list(range(1, p.n + 1))
+    assign = np.array([v > 0 for v in lits[:-1]])
+    assert is_satisfied(golden["p50/literals"], golden["p50/lengths"], assign)
+    s2 = SatSolver([p], precision=1)
+    s2.SetBatchSize(1); s2.SetMaxSteps(1)
+    s2.SetSatStates([0], ics[:1])
+    s2.Solve()
+    s2.WriteResult(0, str(tmp_path / "b.out"))
+    assert (tmp_path / "b.out").read_text().splitlines()[0] == "INDET"
+    tsv = tmp_path / "perf.tsv"
+    s.AppendPerf(0, str(tsv), "p50")
+    s.AppendPerf(1, str(tsv), "p50")
+    rows = [ln.split("\t") for ln in tsv.read_text().splitlines()]
+    assert len(rows) == 2 and all(len(rw) == 7 for rw in rows)
+    assert rows[0][0] == "p50" and rows[0][3] == "solution found"
+    assert int(rows[0][6]) == r["rhs"][0] and float(rows[0][4]) > 0
