@@ -82,12 +82,18 @@ class SatProblem:
         return cls.from_arrays(lits, lens)
 
     @classmethod
-    def read_cnf(cls, path: str) -> "SatProblem":
-        """CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141)."""
+    def read_cnf(cls, path: str, device: int | None = None) -> "SatProblem":
+        """CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141).  With `device`, the
+        clause body is tokenised on that GPU (same results and messages)."""
         h = C.c_void_p()
         msg = C.create_string_buffer(256)
-        check(load().as_problem_read_cnf(path.encode(), C.byref(h), msg, 256))
-        return cls(h)
+        if device is None:
+            check(load().as_problem_read_cnf(path.encode(), C.byref(h), msg, 256))
+        else:
+            check(load().as_problem_read_cnf_device(path.encode(), int(device), C.byref(h), msg, 256))
+        p = cls(h)
+        p.message = msg.value.decode()
+        return p
 
     def write_cnf(self, path: str) -> None:
         """CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74)."""
@@ -297,6 +303,20 @@ class SatSolver:
             st = np.ascontiguousarray(st, np.float64)
             check(self._lib.as_solver_set_states_f64(self._h, _ptr(pi), int(pi.size),
                                                      st.ctypes.data_as(C.c_void_p)))
+
+    IC_DISTRIBUTIONS = {"spin_uniform": 0, "reference": 1}
+
+    def SetRandomInitialState(self, problem_index, seed: int, distribution: str = "spin_uniform",
+                              a0: float = 1.0):
+        """SatSolver::SetRandomInitialState (SatSolver.h:195-201) for a set of
+        trajectories, generated on the device from Philox4x64-10 keyed by seed.
+        "spin_uniform": s ~ U(-1, 1), a = a0 -- for T trajectories of one problem the
+        states equal instances.initial_states(N, M, T, seed, a0);  "reference": the
+        reference's ISat::SetRandomState transform, s = 2u - 1, a = u + 1."""
+        pi = _i32(problem_index)
+        self._traj_problem = pi.copy()
+        check(self._lib.as_solver_set_random_states(self._h, _ptr(pi), int(pi.size), int(seed),
+                                                    self.IC_DISTRIBUTIONS[distribution], float(a0)))
 
     def SetSatState(self, state, problem: int = 0):
         """Single-trajectory form of SatSolver::SetSatState(vector)."""

@@ -36,6 +36,7 @@ SIGNATURES = [
     ("as_device_sm_count", _i32, [_i32]),
     ("as_problem_create", _i32, [_pi32, _pi32, _i32, C.POINTER(_vp)]),
     ("as_problem_read_cnf", _i32, [C.c_char_p, C.POINTER(_vp), C.c_char_p, _i32]),
+    ("as_problem_read_cnf_device", _i32, [C.c_char_p, _i32, C.POINTER(_vp), C.c_char_p, _i32]),
     ("as_problem_write_cnf", _i32, [_vp, C.c_char_p]),
     ("as_problem_get_nmk", _i32, [_vp, _pi32, _pi32, _pi32]),
     ("as_problem_num_literals", _i32, [_vp]),
@@ -64,6 +65,7 @@ SIGNATURES = [
     ("as_solver_set_states_f64", _i32, [_vp, _pi32, _i32, _vp]),
     ("as_solver_set_states_f32", _i32, [_vp, _pi32, _i32, _vp]),
     ("as_solver_set_states_device", _i32, [_vp, _pi32, _i32, _vp, _vp]),
+    ("as_solver_set_random_states", _i32, [_vp, _pi32, _i32, C.c_uint64, _i32, C.c_double]),
     ("as_solver_solve", _i32, [_vp]),
     ("as_solver_solve_async", _i32, [_vp, _vp]),
     ("as_solver_sync", _i32, [_vp]),

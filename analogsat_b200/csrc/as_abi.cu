@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/analogsat_b200.h"
+#include "as_ingest.h"
 #include "as_kernels.cuh"
 #include "as_problem.h"
 #include "as_stream.cuh"
@@ -355,6 +356,61 @@ int32_t as_problem_read_cnf(const char* path, as_problem** out, char* msg, int32
     }
     p->pack_all();
     *out = p;
+    return AS_OK;
+}
+
+int32_t as_problem_read_cnf_device(const char* path, int32_t device, as_problem** out, char* msg,
+                                   int32_t msg_len) {
+    if (!path || !out) return fail(AS_ERR_BAD_INPUT, "as_problem_read_cnf_device: null argument");
+    auto put = [&](const std::string& m) {
+        if (msg && msg_len > 0) {
+            std::strncpy(msg, m.c_str(), msg_len - 1);
+            msg[msg_len - 1] = 0;
+        }
+    };
+    FILE* f = std::fopen(path, "r");
+    if (!f) {
+        put("file open failed");
+        return fail(AS_ERR_IO, "as_problem_read_cnf_device: file open failed");
+    }
+    std::unique_ptr<FILE, int (*)(FILE*)> fg(f, std::fclose);
+    int n = -1, m = -1;
+    std::string mm;
+    if (!read_cnf_header(f, n, m, mm)) {
+        put(mm);
+        return fail(AS_ERR_IO, "as_problem_read_cnf_device: " + mm);
+    }
+    std::unique_ptr<as_problem> p(new as_problem());
+    if (n == 0 || m == 0) {
+        put("empty problem");
+        *out = p.release();
+        return AS_OK;
+    }
+    const long start = std::ftell(f);
+    if (start < 0 || std::fseek(f, 0, SEEK_END) != 0) return fail(AS_ERR_IO, "as_problem_read_cnf_device: seek failed");
+    const long end = std::ftell(f);
+    if (end < start || std::fseek(f, start, SEEK_SET) != 0)
+        return fail(AS_ERR_IO, "as_problem_read_cnf_device: seek failed");
+    const size_t len = (size_t)(end - start);
+    int prev = 0;
+    AS_CUDA(cudaGetDevice(&prev));
+    AS_CUDA(cudaSetDevice(device));
+    struct Restore {
+        int d;
+        ~Restore() { cudaSetDevice(d); }
+    } restore{prev};
+    char* buf = nullptr;  // pinned, so that the body crosses PCIe in one DMA
+    AS_CUDA(cudaMallocHost(&buf, std::max<size_t>(len, 1)));
+    std::unique_ptr<char, cudaError_t (*)(void*)> bg(buf, cudaFreeHost);
+    if (std::fread(buf, 1, len, f) != len) return fail(AS_ERR_IO, "as_problem_read_cnf_device: read failed");
+    std::vector<int32_t> lits, lens;
+    cudaError_t ce = cudaSuccess;
+    const bool ok = asb::parse_cnf_body(buf, len, m, lits, lens, mm, ce);
+    if (ce != cudaSuccess) return fail(AS_ERR_CUDA, "as_problem_read_cnf_device: " + mm);
+    put(mm);
+    if (!ok) return fail(AS_ERR_IO, "as_problem_read_cnf_device: " + mm);
+    p->host.add_clauses(lits.data(), lens.data(), (int)lens.size());
+    *out = p.release();
     return AS_OK;
 }
 
@@ -1253,6 +1309,28 @@ int32_t as_solver_set_states_device(as_solver* s, const int32_t* pi, int32_t nt,
     AS_CUDA(cudaMemcpyAsync(s->states.p, src, (size_t)s->total_values * vb, cudaMemcpyDeviceToDevice,
                             stream ? (cudaStream_t)stream : s->stream));
     if (stream) AS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return AS_OK;
+}
+
+int32_t as_solver_set_random_states(as_solver* s, const int32_t* pi, int32_t nt, uint64_t seed,
+                                    int32_t distribution, double a0) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "as_solver_set_random_states: null solver");
+    if (distribution != AS_IC_SPIN_UNIFORM && distribution != AS_IC_REFERENCE)
+        return fail(AS_ERR_BAD_INPUT, "as_solver_set_random_states: unknown distribution");
+    if (distribution == AS_IC_SPIN_UNIFORM && !(a0 > 0.0 && std::isfinite(a0)))
+        return fail(AS_ERR_BAD_INPUT, "as_solver_set_random_states: need a0 > 0");
+    AS_CUDA(cudaSetDevice(s->device));
+    int r = plan_units(s, pi, nt);
+    if (r) return r;
+    std::vector<asb::IcTraj> tr(nt);
+    for (int t = 0; t < nt; t++) {
+        const auto& q = s->problems[pi[t]];
+        tr[t] = asb::IcTraj{s->traj_off[t], q.n, q.m};
+    }
+    const cudaError_t e = asb::random_states(s->states.p, s->precision == AS_PREC_F64, tr, seed, distribution, a0,
+                                            s->stream);
+    if (e != cudaSuccess)
+        return fail(AS_ERR_CUDA, std::string("as_solver_set_random_states: ") + cudaGetErrorString(e));
     return AS_OK;
 }
 

@@ -32,13 +32,9 @@ void HostProblem::add_clauses(const int32_t* literals, const int32_t* lengths, i
     }
 }
 
-// Same acceptance rules as CnfReader::Read: lines before the "p cnf N M" header are
-// skipped, a header with N == 0 or M == 0 is an empty problem, then exactly M
-// zero-terminated clauses must follow.
-bool read_cnf(const char* path, HostProblem& p, std::string& msg) {
-    FILE* f = std::fopen(path, "r");
-    if (!f) { msg = "file open failed"; return false; }
-    int n = -1, m = -1;
+bool read_cnf_header(std::FILE* f, int& n, int& m, std::string& msg) {
+    n = -1;
+    m = -1;
     char line[1024];
     while (!std::feof(f)) {
         int c = std::fgetc(f);
@@ -46,29 +42,45 @@ bool read_cnf(const char* path, HostProblem& p, std::string& msg) {
         if (c == 'p') {
             if (std::fscanf(f, " cnf %d %d", &n, &m) == 2) break;
             msg = "expected: p cnf <variables> <clauses>";
-            std::fclose(f);
             return false;
         }
         if (c != '\n' && !std::fgets(line, sizeof(line), f)) break;
     }
-    if (n < 0 || m < 0) { msg = "could not find a SAT declaration"; std::fclose(f); return false; }
+    if (n < 0 || m < 0) { msg = "could not find a SAT declaration"; return false; }
+    return true;
+}
+
+// Same acceptance rules as CnfReader::Read: lines before the "p cnf N M" header are
+// skipped, a header with N == 0 or M == 0 is an empty problem, then exactly M
+// zero-terminated clauses must follow.  Literals are read as long and must lie within
+// +-(2^31 - 1): the reference's "%d" leaves larger values undefined.
+bool read_cnf(const char* path, HostProblem& p, std::string& msg) {
+    FILE* f = std::fopen(path, "r");
+    if (!f) { msg = "file open failed"; return false; }
+    int n = -1, m = -1;
+    if (!read_cnf_header(f, n, m, msg)) { std::fclose(f); return false; }
     p = HostProblem();
     if (n == 0 || m == 0) { msg = "empty problem"; std::fclose(f); return true; }
     std::vector<int32_t> lits, lens;
-    lits.reserve((size_t)m * 3);
-    lens.reserve(m);
+    lits.reserve(std::min<size_t>((size_t)m * 3, (size_t)1 << 24));  // the header may overstate M
+    lens.reserve(std::min<size_t>((size_t)m, (size_t)1 << 22));
     int read = 0;
     while (read < m) {
         int len = 0;
         while (true) {
-            int lit;
-            if (std::fscanf(f, "%d", &lit) != 1) {
+            long lit;
+            if (std::fscanf(f, "%ld", &lit) != 1) {
                 msg = "expected more literals in file";
                 std::fclose(f);
                 return false;
             }
+            if (lit > 2147483647L || lit < -2147483647L) {
+                msg = "literal out of range";
+                std::fclose(f);
+                return false;
+            }
             if (lit == 0) break;
-            lits.push_back(lit);
+            lits.push_back((int32_t)lit);
             len++;
         }
         lens.push_back(len);

@@ -45,6 +45,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -62,6 +63,10 @@ struct HostProblem {
 
 // CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141).  Returns false and fills msg on error.
 bool read_cnf(const char* path, HostProblem& p, std::string& msg);
+// The preamble part of CnfReader::Read (CnfReader.cpp:54-91): skips lines up to the
+// "p cnf N M" declaration and leaves f just after M.  Returns false with msg set when
+// the declaration is malformed or missing.
+bool read_cnf_header(std::FILE* f, int& n, int& m, std::string& msg);
 // CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74).
 bool write_cnf(const char* path, const HostProblem& p);
 

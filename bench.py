@@ -64,12 +64,13 @@ def parse_args():
     ap.add_argument("--all-trajectories", action="store_true",
                     help="run every trajectory to its own SatResult (no early exit per instance)")
     ap.add_argument("--workload", default="planted1000",
-                    choices=["planted1000", "uneven", "maxsat", "adjoint"],
+                    choices=["planted1000", "uneven", "maxsat", "adjoint", "ingest"],
                     help="planted1000: the headline configuration; uneven: 512 planted instances "
                          "N~U{100..5000}, alpha~U(3.8,4.26), 64 trajectories each, one graph-captured "
                          "launch; maxsat: one random 4-SAT N=1e5, M=1e6 instance, 32 trajectories, "
                          "minimise unsat over --maxsat-seconds; adjoint: gradients of V at T=5 for "
-                         "1024 random 3-SAT N=200, M=850 instances, FP32 vs FP64")
+                         "1024 random 3-SAT N=200, M=850 instances, FP32 vs FP64; ingest: GPU CNF "
+                         "reader on the N=1e5, M=1e6 file and device-generated initial states")
     ap.add_argument("--maxsat-seconds", type=float, default=60.0)
     ap.add_argument("--maxsat-steps", type=int, default=0,
                     help="maxsat workload: stop every trajectory after this many steps (0: budget only)")
@@ -577,6 +578,65 @@ def run_adjoint(args):
                       "mean_loss_after_a0_step": float(g2["loss"].mean())}), flush=True)
 
 
+def run_ingest(args):
+    """Device-side ingest at the large-instance size.  CNF: the random 4-SAT instance
+    N=1e5, M=1e6 as a DIMACS file (about 27 MB) read by the host reader, by the
+    reference's CnfReader (CPU baseline, when built) and by the GPU tokeniser; wall
+    time of each complete read (file to host clause arrays).  Initial states: the FP32
+    batch of 64 x 256 trajectories of N=1000, M=4250 (86M values, 344 MB) generated in
+    HBM, against numpy's generator plus the host-to-device copy."""
+    import shutil
+    import analogsat_b200 as A
+    from analogsat_b200.instances import make_instance, initial_states
+
+    def best_of(fn, reps):
+        t = []
+        for _ in range(max(1, reps)):
+            t0 = time.perf_counter()
+            fn()
+            t.append(time.perf_counter() - t0)
+        return min(t)
+
+    lits, lens, _ = make_instance("fast", 100_000, 1_000_000, 4, seed=5000)
+    d = tempfile.mkdtemp()
+    try:
+        f = os.path.join(d, "random-4sat-N1e5-M1e6.cnf")
+        A.SatProblem.from_arrays(lits, lens).write_cnf(f)
+        size = os.path.getsize(f)
+        q = A.SatProblem.read_cnf(f, device=0)  # warm-up, and the exactness check
+        ql, qn = q.GetAllClauses()
+        assert np.array_equal(ql, lits) and np.array_equal(qn, lens)
+        dev = best_of(lambda: A.SatProblem.read_cnf(f, device=0), args.steps)
+        host = best_of(lambda: A.SatProblem.read_cnf(f), 2)
+        ref = None
+        if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libanalogsat_ref.so")):
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            from oracle import Reference
+            R = Reference()
+            ref = best_of(lambda: R.read_cnf(f), 1)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    n, m, T = 1000, 4250, 64 * 256
+    pl, pn, _ = make_instance("planted", n, m, 3, seed=2000)
+    s = A.SatSolver([A.SatProblem.from_arrays(pl, pn)], precision=0)
+    pidx = np.zeros(T, np.int32)
+    s.SetRandomInitialState(pidx, seed=1)  # warm-up (allocates the state buffer)
+    ic_dev = best_of(lambda: s.SetRandomInitialState(pidx, seed=1), args.steps)
+
+    def host_path():
+        s.SetSatStates(pidx, initial_states(n, m, T, seed=1, dtype=np.float32))
+    ic_host = best_of(host_path, 2)
+    vals = T * (n + m)
+    print(json.dumps({"workload": "ingest-cnf-random-4sat-N1e5-M1e6-and-states-64x256-N1000-M4250",
+                      "cnf_bytes": size, "cnf_read_s": {"device": dev, "host": host, "reference": ref},
+                      "cnf_device_GB_per_s": size / dev / 1e9,
+                      "states": {"values": vals, "bytes_fp32": 4 * vals, "device_s": ic_dev,
+                                 "numpy_plus_h2d_s": ic_host,
+                                 "device_GB_per_s": 4 * vals / ic_dev / 1e9},
+                      "note": "wall time per complete call through the C ABI, best of the repeats; "
+                              "kernel shares in profiles/ingest_kernels_cnf_N1e5_M1e6.md"}), flush=True)
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -587,6 +647,8 @@ def main():
         run_maxsat(args)
     elif args.workload == "adjoint":
         run_adjoint(args)
+    elif args.workload == "ingest":
+        run_ingest(args)
     else:
         run_ours(args)
 

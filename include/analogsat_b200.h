@@ -71,8 +71,16 @@ int32_t as_device_sm_count(int32_t device);
 int32_t as_problem_create(const int32_t* literals, const int32_t* lengths, int32_t num_clauses,
                           as_problem** out);
 
-/* CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141); msg receives the reader's message. */
+/* CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141); msg receives the reader's message.
+ * Literals beyond +-(2^31 - 1) fail with "literal out of range". */
 int32_t as_problem_read_cnf(const char* path, as_problem** out, char* msg, int32_t msg_len);
+/* The same reader for very large files: the preamble is read on the host, the clause
+ * body is copied once to `device` and tokenised there (every maximal run of digits is
+ * one literal; the first malformed byte, sign without digits, end of file or
+ * out-of-range literal before the M-th zero fails).  Results, messages and error
+ * codes are those of as_problem_read_cnf. */
+int32_t as_problem_read_cnf_device(const char* path, int32_t device, as_problem** out, char* msg,
+                                   int32_t msg_len);
 
 /* CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74). */
 int32_t as_problem_write_cnf(const as_problem* p, const char* path);
@@ -171,6 +179,22 @@ int32_t as_solver_set_states_f32(as_solver* s, const int32_t* problem_index, int
  * float for AS_PREC_F32_LOGA, double for AS_PREC_F64), copied device-to-device. */
 int32_t as_solver_set_states_device(as_solver* s, const int32_t* problem_index, int32_t num_traj,
                                     const void* states_dev, void* stream);
+
+/* SatSolver::SetRandomInitialState (SatSolver.h:195-201; ISat::SetRandomState,
+ * CpuSat.cpp:123-133, CudaSat1.cu:452-464) for a set of trajectories, generated in
+ * device memory (no host state, no host-to-device copy of it).  Uniforms u in [0, 1)
+ * come from Philox4x64-10 keyed by (seed, 0): draw d is output d%4 of the block with
+ * counter d/4 + 1, u = (x >> 11) * 2^-53 -- the stream of numpy's
+ * Generator(Philox(key=seed)) -- and the trajectories draw from it in order.
+ *   AS_IC_SPIN_UNIFORM: N draws per trajectory, s = 2u - 1, a_m = a0 (> 0); T equal
+ *     trajectories get numpy's .uniform(-1, 1, (T, N)) row by row.
+ *   AS_IC_REFERENCE: N + M draws, s = 2u - 1, a = u + 1 (the reference's transform,
+ *     KernelSetInitial1, CudaSatBase.cu:37-55); a0 is ignored.
+ * FP32 solvers store each value rounded to nearest from double. */
+#define AS_IC_SPIN_UNIFORM 0
+#define AS_IC_REFERENCE 1
+int32_t as_solver_set_random_states(as_solver* s, const int32_t* problem_index, int32_t num_traj,
+                                    uint64_t seed, int32_t distribution, double a0);
 
 /* SatSolver::Solve (SatSolver.h:162-165, DoSolve 273-355) for every trajectory, in
  * one persistent launch.  Blocks until done.  Per-trajectory results via

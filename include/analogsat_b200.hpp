@@ -98,11 +98,13 @@ public:
     // SatProblem::Clear
     void Clear() { lits_.clear(); lens_.clear(); h_.reset(); }
 
-    // CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141)
-    static SatProblem ReadCnf(const std::string& path) {
+    // CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141); with device >= 0 the clause
+    // body is tokenised on that GPU (as_problem_read_cnf_device, same results).
+    static SatProblem ReadCnf(const std::string& path, int device = -1) {
         as_problem* h = nullptr;
         char msg[256];
-        check(as_problem_read_cnf(path.c_str(), &h, msg, sizeof(msg)));
+        check(device >= 0 ? as_problem_read_cnf_device(path.c_str(), device, &h, msg, sizeof(msg))
+                          : as_problem_read_cnf(path.c_str(), &h, msg, sizeof(msg)));
         SatProblem p;
         p.h_.reset(h, as_problem_free);
         const int32_t nl = as_problem_num_literals(h);
@@ -232,6 +234,15 @@ public:
         index_ = problem_index;
     }
 
+    // SatSolver::SetRandomInitialState (SatSolver.h:195-201) for every trajectory, generated
+    // on the device from Philox4x64-10 keyed by seed (as_solver_set_random_states).
+    void SetRandomInitialState(const std::vector<int32_t>& problem_index, uint64_t seed,
+                               int32_t distribution = AS_IC_REFERENCE, double a0 = 1.0) {
+        check(as_solver_set_random_states(s_.get(), problem_index.data(), (int32_t)problem_index.size(), seed,
+                                          distribution, a0));
+        index_ = problem_index;
+    }
+
     // Runs every trajectory to its SatResult; returns them in trajectory order.
     std::vector<SatResult> Solve() {
         const auto t0 = std::chrono::steady_clock::now();
@@ -343,6 +354,13 @@ public:
         const SatResult r = batch_->Solve()[0];
         state_ = batch_->GetSatState(0);
         return r;
+    }
+
+    // SatSolver::SetRandomInitialState (SatSolver.h:195-201): the reference's transform
+    // (s = 2u - 1, a = u + 1) of Philox uniforms keyed by seed, drawn on the device.
+    void SetRandomInitialState(uint64_t seed) {
+        need().SetRandomInitialState({0}, seed, AS_IC_REFERENCE);
+        state_ = batch_->GetSatState(0);
     }
 
     SatStateView<TFloat> GetSatState() const { return SatStateView<TFloat>(state_); }

@@ -73,6 +73,15 @@ int main(int argc, char** argv) {
         while (in >> v) ic.push_back(v);
         solve_one<double>(p, ic, "f64");
         solve_one<float>(p, ic, "f32");
+        // the GPU CNF reader gives the same problem; device-generated initial state
+        SatProblem q = SatProblem::ReadCnf(argv[2], 0);
+        std::printf("cnf_device %d %d %d\n", q.Get_N(), q.Get_M(), q.Get_K());
+        SatSolver<double> s;
+        s.SetProblem(q);
+        s.SetRandomInitialState(42);
+        std::vector<double> x;
+        s.GetSatState().CopyTo(x);
+        std::printf("rand %zu %.17g %.17g %.17g\n", x.size(), x[0], x[q.Get_N() - 1], x.back());
         return 0;
     }
     std::fprintf(stderr, "usage: adapter_check host <dir> | gpu <cnf> <ic>\n");

@@ -43,3 +43,7 @@ def test_adapter_solves_like_reference(adapter_bin, tmp_path, golden):
     assert int(rows["f64"][1]) == golden["p50/solve_steps"][0]
     assert int(rows["f64"][2]) == golden["p50/solve_rhs"][0]
     assert int(rows["f32"][0]) == 0 and int(rows["f32"][4]) == 0
+    assert [int(v) for v in rows["cnf_device"]] == [50, 210, 3]
+    u = np.random.Generator(np.random.Philox(key=42)).random(260)  # reference transform
+    assert int(rows["rand"][0]) == 260
+    assert [float(v) for v in rows["rand"][1:]] == [u[0] * 2 - 1, u[49] * 2 - 1, u[259] + 1]
