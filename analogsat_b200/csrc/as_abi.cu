@@ -399,17 +399,13 @@ int32_t as_problem_read_cnf_device(const char* path, int32_t device, as_problem*
         int d;
         ~Restore() { cudaSetDevice(d); }
     } restore{prev};
-    char* buf = nullptr;  // pinned, so that the body crosses PCIe in one DMA
-    AS_CUDA(cudaMallocHost(&buf, std::max<size_t>(len, 1)));
-    std::unique_ptr<char, cudaError_t (*)(void*)> bg(buf, cudaFreeHost);
-    if (std::fread(buf, 1, len, f) != len) return fail(AS_ERR_IO, "as_problem_read_cnf_device: read failed");
     std::vector<int32_t> lits, lens;
     cudaError_t ce = cudaSuccess;
-    const bool ok = asb::parse_cnf_body(buf, len, m, lits, lens, mm, ce);
+    const bool ok = asb::parse_cnf_body(f, len, m, lits, lens, mm, ce);
     if (ce != cudaSuccess) return fail(AS_ERR_CUDA, "as_problem_read_cnf_device: " + mm);
     put(mm);
     if (!ok) return fail(AS_ERR_IO, "as_problem_read_cnf_device: " + mm);
-    p->host.add_clauses(lits.data(), lens.data(), (int)lens.size());
+    p->host.set_clauses(std::move(lits), lens);
     *out = p.release();
     return AS_OK;
 }

@@ -63,69 +63,85 @@ template <typename T> __device__ __forceinline__ T narrow(double v);
 template <> __device__ __forceinline__ double narrow<double>(double v) { return v; }
 template <> __device__ __forceinline__ float narrow<float>(double v) { return __double2float_rn(v); }
 
-// Last trajectory whose first draw (or fill element) is <= d.
-__device__ __forceinline__ int find_traj(const long long* __restrict__ first, int nt, long long d) {
-    int lo = 0, hi = nt - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (first[mid] <= d) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
+// Per trajectory on the device: state offset, first draw of the stream, N and M.
+struct IcRow {
+    long long off, draw;
+    int n, m;
+};
 
-// One thread per Philox block: draws 4b .. 4b+3 of the stream, written to the
-// trajectories (and elements) they belong to.  draw[] holds nt + 1 entries.
+constexpr int kIcChunk = 1024;    // draws per CTA of ic_draw_kernel
+constexpr int kFillChunk = 8192;  // constant elements per CTA of ic_fill_kernel
+
+// Grid (chunks, trajectories): CTA (x, y) takes draws [x * kIcChunk, +kIcChunk) of
+// trajectories y, y + gridDim.y, ...  It computes the Philox blocks covering them (one
+// per thread), stages the values in shared memory and stores them with consecutive
+// threads on consecutive elements.
 template <typename T>
-__global__ void __launch_bounds__(256) ic_draw_kernel(T* __restrict__ states, const IcTraj* __restrict__ tr,
-                                                      const long long* __restrict__ draw, int nt, long long ndraw,
+__global__ void __launch_bounds__(256) ic_draw_kernel(T* __restrict__ states, const IcRow* __restrict__ rows, int nt,
                                                       unsigned long long seed, int dist) {
-    const long long nblk = (ndraw + 3) >> 2;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nblk; b += stride) {
-        unsigned long long r[4];
-        philox4x64_10((unsigned long long)b + 1ull, seed, r);
-        const long long d0 = b << 2;
-        int t = find_traj(draw, nt, d0);
+    __shared__ T vals[kIcChunk];
+    for (int t = blockIdx.y; t < nt; t += gridDim.y) {
+        const IcRow R = rows[t];
+        const long long j0 = (long long)blockIdx.x * kIcChunk;
+        const long long ndraw = R.n + (dist == kIcSpinUniform ? 0 : (long long)R.m);
+        if (j0 >= ndraw) continue;  // uniform across the CTA
+        const int cnt = (int)min((long long)kIcChunk, ndraw - j0);
+        const long long d0 = R.draw + j0;
+        const long long b0 = d0 >> 2;
+        const int nb = (int)(((d0 + cnt - 1) >> 2) - b0 + 1);
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+            unsigned long long r[4];
+            philox4x64_10((unsigned long long)(b0 + i) + 1ull, seed, r);
+            const long long e0 = ((b0 + i) << 2) - d0;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const long long d = d0 + i;
-            if (d >= ndraw) break;
-            while (draw[t + 1] <= d) t++;
-            const long long j = d - draw[t];
-            const double u = (double)(r[i] >> 11) * 0x1.0p-53;
-            const double v = (dist == kIcSpinUniform || j < tr[t].n) ? __dadd_rn(__dmul_rn(u, 2.0), -1.0)
-                                                                    : __dadd_rn(u, 1.0);
-            states[tr[t].off + j] = narrow<T>(v);
+            for (int k = 0; k < 4; k++) {
+                const long long e = e0 + k;
+                if (e < 0 || e >= cnt) continue;
+                const double u = (double)(r[k] >> 11) * 0x1.0p-53;
+                const bool spin = dist == kIcSpinUniform || j0 + e < R.n;
+                vals[e] = narrow<T>(spin ? __dadd_rn(__dmul_rn(u, 2.0), -1.0) : __dadd_rn(u, 1.0));
+            }
         }
+        __syncthreads();
+        T* dst = states + R.off + j0;
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) dst[e] = vals[e];
+        __syncthreads();
     }
 }
 
-// a_m = a0 for every trajectory (kIcSpinUniform); fill[] holds nt + 1 prefix entries
-// of M.  Eight consecutive elements per thread.
+// a_m = a0 (kIcSpinUniform).  Grid (chunks, trajectories): CTA (x, y) fills weights
+// [x * kFillChunk, +kFillChunk) of trajectories y, y + gridDim.y, ... with 16-byte
+// stores between a scalar head and tail; the next trajectory's row is loaded before
+// the current stores are issued.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static __device__ float4 splat(float v) { return make_float4(v, v, v, v); } };
+template <> struct Vec16<double> { using type = double2; static __device__ double2 splat(double v) { return make_double2(v, v); } };
+
 template <typename T>
-__global__ void __launch_bounds__(256) ic_fill_kernel(T* __restrict__ states, const IcTraj* __restrict__ tr,
-                                                      const long long* __restrict__ fill, int nt, long long total, T a0) {
-    const long long nchunk = (total + 7) >> 3;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nchunk; c += stride) {
-        const long long e0 = c << 3;
-        int t = find_traj(fill, nt, e0);
-        for (int i = 0; i < 8; i++) {
-            const long long e = e0 + i;
-            if (e >= total) break;
-            while (fill[t + 1] <= e) t++;
-            states[tr[t].off + tr[t].n + (e - fill[t])] = a0;
+__global__ void __launch_bounds__(256) ic_fill_kernel(T* __restrict__ states, const IcRow* __restrict__ rows, int nt,
+                                                      T a0) {
+    using V = typename Vec16<T>::type;
+    constexpr int kPer = 16 / sizeof(T);
+    const V v = Vec16<T>::splat(a0);
+    int t = blockIdx.y;
+    if (t >= nt) return;
+    IcRow R = rows[t];
+    for (; t < nt; t += gridDim.y) {
+        const IcRow Rn = t + (int)gridDim.y < nt ? rows[t + gridDim.y] : R;
+        const long long j0 = (long long)blockIdx.x * kFillChunk;
+        if (j0 < R.m) {
+            const int cnt = (int)min((long long)kFillChunk, (long long)R.m - j0);
+            T* dst = states + R.off + R.n + j0;
+            const int head = min(cnt, (int)(((16u - ((unsigned)(uintptr_t)dst & 15u)) & 15u) / sizeof(T)));
+            if ((int)threadIdx.x < head) dst[threadIdx.x] = a0;
+            const int nvec = (cnt - head) / kPer;
+            V* vd = reinterpret_cast<V*>(dst + head);
+            for (int i = threadIdx.x; i < nvec; i += blockDim.x) vd[i] = v;
+            const int done = head + nvec * kPer;
+            if ((int)threadIdx.x < cnt - done) dst[done + threadIdx.x] = a0;
         }
+        R = Rn;
     }
-}
-
-int grid_for(long long work, int block) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long want = (work + block - 1) / block;
-    return (int)std::max(1ll, std::min(want, (long long)sms * 8));
 }
 
 struct Dev {
@@ -143,68 +159,122 @@ struct CnfHeader {
     long long pos_m;          // position of the M-th zero (-1: not reached)
 };
 
-__device__ __forceinline__ bool is_digit(int c) { return c >= '0' && c <= '9'; }
-__device__ __forceinline__ bool is_space(int c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
+// Byte classes of four bytes at once: each returns 0x80 in the bytes where the class
+// holds (C locale: white space is ' ' and '\t'..'\r').
+__device__ __forceinline__ unsigned cls_digit(unsigned w) { return __vcmpltu4(__vsub4(w, 0x30303030u), 0x0a0a0a0au) & 0x80808080u; }
+__device__ __forceinline__ unsigned cls_nonzero(unsigned w) { return __vcmpltu4(__vsub4(w, 0x31313131u), 0x09090909u) & 0x80808080u; }
+__device__ __forceinline__ unsigned cls_space(unsigned w) {
+    return (__vcmpeq4(w, 0x20202020u) | __vcmpltu4(__vsub4(w, 0x09090909u), 0x05050505u)) & 0x80808080u;
+}
+__device__ __forceinline__ unsigned cls_minus(unsigned w) { return __vcmpeq4(w, 0x2d2d2d2du) & 0x80808080u; }
+__device__ __forceinline__ unsigned cls_sign(unsigned w) { return (__vcmpeq4(w, 0x2b2b2b2bu) & 0x80808080u) | cls_minus(w); }
+// 0x80 flags of four bytes -> bits 0..3 (byte 0 -> bit 0)
+__device__ __forceinline__ unsigned pack4(unsigned f) { return ((f >> 7) * 0x10204080u) >> 28; }
 
-// Shared-memory tile: sb[16 + i] = body[base + i]; sb[15] and sb[16 + kCnfTile] are
-// the bytes on either side.
-struct CnfTile {
-    const unsigned char* body;
-    long long len, base;
-    const unsigned char* sb;
-    // Byte at q; -1 outside the body (before it: no digit can precede the body, since
-    // the header's last number was read greedily; after it: end of file).
-    __device__ __forceinline__ int at(long long q) const {
-        if (q < 0 || q >= len) return -1;
-        const long long r = q - base;
-        if (r >= -1 && r <= kCnfTile) return sb[16 + r];
-        return __ldg(body + q);
-    }
-};
-
-__device__ void stage_tile(const unsigned char* __restrict__ body, long long len, long long base, unsigned char* sb) {
-    const int t = threadIdx.x;
-    const long long p = base + (long long)t * kCnfBytes;
-    if (p + kCnfBytes <= len) {
-        *reinterpret_cast<uint4*>(sb + 16 + t * kCnfBytes) = __ldg(reinterpret_cast<const uint4*>(body + p));
-    } else {
-        for (int i = 0; i < kCnfBytes; i++) sb[16 + t * kCnfBytes + i] = p + i < len ? body[p + i] : 0;
-    }
-    if (t == 0) sb[15] = base > 0 ? body[base - 1] : ' ';
-    if (t == 1) sb[16 + kCnfTile] = base + kCnfTile < len ? body[base + kCnfTile] : 0;
+template <unsigned (*F)(unsigned)>
+__device__ __forceinline__ unsigned mask16(const uint4& v) {
+    return pack4(F(v.x)) | pack4(F(v.y)) << 4 | pack4(F(v.z)) << 8 | pack4(F(v.w)) << 12;
 }
 
-// Scans this thread's 16 bytes.  For each literal (run of digits starting here) calls
-// emit(position, value, negative, zero); returns the packed counts tokens << 16 | zeros
-// and lowers fail to the first failure seen.
-template <typename F>
-__device__ __forceinline__ int scan_bytes(const CnfTile& T, long long p0, unsigned long long& fail, F&& emit) {
+// Byte i (0..31) of a thread's own 16 bytes followed by the next 16.
+__device__ __forceinline__ int byte_at(const uint4& a, const uint4& b, int i) {
+    const int k = i >> 2;
+    unsigned w = a.x;
+    w = k == 1 ? a.y : w;
+    w = k == 2 ? a.z : w;
+    w = k == 3 ? a.w : w;
+    w = k == 4 ? b.x : w;
+    w = k == 5 ? b.y : w;
+    w = k == 6 ? b.z : w;
+    w = k == 7 ? b.w : w;
+    return (w >> ((i & 3) * 8)) & 0xff;
+}
+
+// Shared-memory tile: sb[16 + i] = body[base + i] for i < kCnfTile + 16 (the tile and
+// the 16 bytes after it); sb[15] = the byte before (' ' for the first tile).
+__device__ void stage_tile(const unsigned char* __restrict__ body, long long len, long long base, unsigned char* sb) {
+    for (int c = threadIdx.x; c < kCnfTile / 16 + 1; c += blockDim.x) {
+        const long long p = base + 16ll * c;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (p + 16 <= len) {
+            v = __ldg(reinterpret_cast<const uint4*>(body + p));
+        } else if (p < len) {
+            unsigned char t[16];
+            for (int i = 0; i < 16; i++) t[i] = p + i < len ? body[p + i] : 0;
+            memcpy(&v, t, 16);
+        }
+        *reinterpret_cast<uint4*>(sb + 16 + 16 * c) = v;
+    }
+    if (threadIdx.x == 0) sb[15] = base > 0 ? body[base - 1] : ' ';
+}
+
+// A literal (maximal run of digits) starting at byte q of the body, scanned in global
+// memory: its value (saturated), whether it is zero and whether it is out of range.
+__device__ void scan_long(const unsigned char* __restrict__ body, long long len, long long q, long long& v, bool& range) {
+    v = 0;
+    range = false;
+    for (long long r = q; r < len; r++) {
+        const int d = body[r];
+        if (d < '0' || d > '9') break;
+        if (!range) {
+            v = v * 10 + (d - '0');
+            range = v > INT_MAX;
+        }
+    }
+}
+
+// Scans one thread's 16 bytes at body position p0 (own: those bytes, next: the 16
+// after them, prev: the byte before).  For each literal starting here calls
+// emit(position, value, negative, zero) (value only when VALUES); returns the packed counts tokens << 16 |
+// zeros and lowers fail to the first failure among these bytes.
+template <bool VALUES, typename F>
+__device__ __forceinline__ int scan_bytes(const unsigned char* __restrict__ body, long long len, long long p0,
+                                          const uint4& own, const uint4& next, int prev, unsigned long long& fail,
+                                          F&& emit) {
+    const long long avail = len - p0;
+    if (avail <= 0) return 0;
+    const unsigned valid = avail >= 32 ? 0xffffffffu : (1u << avail) - 1u;
+    const unsigned dig = (mask16<cls_digit>(own) | mask16<cls_digit>(next) << 16) & valid;
+    const unsigned nz = (mask16<cls_nonzero>(own) | mask16<cls_nonzero>(next) << 16) & valid;
+    const unsigned sp = mask16<cls_space>(own) & valid;
+    const unsigned sg = mask16<cls_sign>(own) & valid;
+    const unsigned mn = mask16<cls_minus>(own) & valid;
+    const unsigned prev_dig = (prev >= '0' && prev <= '9') ? 1u : 0u;
+    const unsigned prev_mn = prev == '-' ? 1u : 0u;
+    // failures: a byte of no class, a sign without a digit right after it
+    const unsigned bad = ((~(dig | sp | sg) & valid) | (sg & ~(dig >> 1))) & 0xffffu;
+    if (bad) fail = min(fail, (unsigned long long)(p0 + __ffs(bad) - 1) << 1);
+    unsigned starts = dig & ~((dig << 1) | prev_dig) & 0xffffu;
     int tok = 0, zero = 0;
-    for (int i = 0; i < kCnfBytes; i++) {
-        const long long q = p0 + i;
-        if (q >= T.len) break;
-        const int c = T.at(q);
-        if (is_digit(c)) {
-            if (is_digit(T.at(q - 1))) continue;  // inside a literal that started earlier
-            long long v = 0;
-            bool range = false;
-            for (long long r = q;; r++) {
-                const int d = T.at(r);
-                if (!is_digit(d)) break;
-                if (!range) {
-                    v = v * 10 + (d - '0');
+    while (starts) {
+        const int s = __ffs(starts) - 1;
+        starts &= starts - 1;
+        const unsigned rest = ~(dig >> s);  // bit j: byte s + j is not a digit
+        const int e = rest ? s + __ffs(rest) - 1 : 32;
+        long long v = 0;
+        bool range = false, is_zero;
+        if (e >= 32) {  // the run may continue past the 32 bytes in registers
+            scan_long(body, len, p0 + s, v, range);
+            is_zero = v == 0;
+        } else {
+            const unsigned run = (1u << (e - s)) - 1u;
+            const unsigned nzr = (nz >> s) & run;
+            is_zero = nzr == 0;
+            if (!is_zero) {
+                const int sig = e - s - (__ffs(nzr) - 1);  // digits after the leading zeros
+                if (sig > 10) {
+                    range = true;
+                } else if (VALUES || sig == 10) {  // ten digits may still exceed 2^31 - 1
+                    for (int i = e - sig; i < e; i++) v = v * 10 + (byte_at(own, next, i) - '0');
                     range = v > INT_MAX;
                 }
             }
-            if (range) fail = min(fail, ((unsigned long long)q << 1) | 1ull);
-            emit(q, range ? 0 : (int)v, T.at(q - 1) == '-', v == 0);
-            tok++;
-            zero += v == 0;
-        } else if (c == '+' || c == '-') {
-            if (!is_digit(T.at(q + 1))) fail = min(fail, (unsigned long long)q << 1);
-        } else if (!is_space(c)) {
-            fail = min(fail, (unsigned long long)q << 1);
         }
+        if (range) fail = min(fail, ((unsigned long long)(p0 + s) << 1) | 1ull);
+        const bool neg = s ? ((mn >> (s - 1)) & 1u) : prev_mn;
+        emit(p0 + s, range ? 0 : (int)v, neg, is_zero);
+        tok++;
+        zero += is_zero;
     }
     return (tok << 16) | zero;
 }
@@ -223,9 +293,12 @@ __global__ void __launch_bounds__(kCnfThreads) cnf_count_kernel(const unsigned c
     const long long base = (long long)blockIdx.x * kCnfTile;
     stage_tile(body, len, base, sb);
     __syncthreads();
-    const CnfTile T{body, len, base, sb};
+    const int tid = threadIdx.x;
+    const uint4 own = *reinterpret_cast<const uint4*>(sb + 16 + kCnfBytes * tid);
+    const uint4 next = *reinterpret_cast<const uint4*>(sb + 32 + kCnfBytes * tid);
     unsigned long long fail = kNoFail;
-    int c = scan_bytes(T, base + (long long)threadIdx.x * kCnfBytes, fail, [](long long, int, bool, bool) {});
+    int c = scan_bytes<false>(body, len, base + (long long)kCnfBytes * tid, own, next, sb[15 + kCnfBytes * tid], fail,
+                       [](long long, int, bool, bool) {});
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     fail = warp_min64(fail);
@@ -296,10 +369,13 @@ __global__ void __launch_bounds__(kCnfThreads) cnf_emit_kernel(const unsigned ch
     const long long base = (long long)blockIdx.x * kCnfTile;
     stage_tile(body, len, base, sb);
     __syncthreads();
-    const CnfTile T{body, len, base, sb};
-    const long long p0 = base + (long long)threadIdx.x * kCnfBytes;
+    const int tid = threadIdx.x;
+    const uint4 own = *reinterpret_cast<const uint4*>(sb + 16 + kCnfBytes * tid);
+    const uint4 next = *reinterpret_cast<const uint4*>(sb + 32 + kCnfBytes * tid);
+    const int prev = sb[15 + kCnfBytes * tid];
+    const long long p0 = base + (long long)kCnfBytes * tid;
     unsigned long long fail = kNoFail;
-    const int c = scan_bytes(T, p0, fail, [](long long, int, bool, bool) {});
+    const int c = scan_bytes<false>(body, len, p0, own, next, prev, fail, [](long long, int, bool, bool) {});
     // exclusive block scan of the packed counts
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int inc = c;
@@ -315,7 +391,7 @@ __global__ void __launch_bounds__(kCnfThreads) cnf_emit_kernel(const unsigned ch
     const int ex = before + inc - c;
     long long k = tok_pre[blockIdx.x] + (ex >> 16);
     long long z = zero_pre[blockIdx.x] + (ex & 0xffff);
-    scan_bytes(T, p0, fail, [&](long long q, int v, bool neg, bool is_zero) {
+    scan_bytes<true>(body, len, p0, own, next, prev, fail, [&](long long q, int v, bool neg, bool is_zero) {
         if (z < m) {
             if (is_zero) {
                 ends[z] = (int)(k - z);
@@ -335,41 +411,48 @@ cudaError_t random_states(void* states, bool f64, const std::vector<IcTraj>& tra
                           int distribution, double a0, cudaStream_t stream) {
     const int nt = (int)traj.size();
     if (nt == 0) return cudaSuccess;
-    // prefix tables (with a sentinel) of the draws and of the constant elements
-    std::vector<long long> draw(nt + 1, 0), fill(nt + 1, 0);
+    // per trajectory: offset, first draw, N, M; the longest draw and weight runs
+    std::vector<IcRow> rows(nt);
+    long long draw = 0, max_draw = 0, max_m = 0;
+    const bool spin_only = distribution == kIcSpinUniform;
     for (int t = 0; t < nt; t++) {
-        const bool spin_only = distribution == kIcSpinUniform;
-        draw[t + 1] = draw[t] + traj[t].n + (spin_only ? 0 : traj[t].m);
-        fill[t + 1] = fill[t] + (spin_only ? traj[t].m : 0);
+        const long long nd = traj[t].n + (spin_only ? 0 : (long long)traj[t].m);
+        rows[t] = IcRow{traj[t].off, draw, traj[t].n, traj[t].m};
+        draw += nd;
+        max_draw = std::max(max_draw, nd);
+        max_m = std::max(max_m, (long long)traj[t].m);
     }
-    Dev dt, dd, df;
-    const size_t tb = sizeof(IcTraj) * nt, lb = sizeof(long long) * (nt + 1);
+    Dev dr;
+    const size_t rb = sizeof(IcRow) * nt;
     cudaError_t e;
-    if ((e = cudaMalloc(&dt.p, tb)) || (e = cudaMalloc(&dd.p, lb)) || (e = cudaMalloc(&df.p, lb))) return e;
-    if ((e = cudaMemcpyAsync(dt.p, traj.data(), tb, cudaMemcpyHostToDevice, stream)) ||
-        (e = cudaMemcpyAsync(dd.p, draw.data(), lb, cudaMemcpyHostToDevice, stream)) ||
-        (e = cudaMemcpyAsync(df.p, fill.data(), lb, cudaMemcpyHostToDevice, stream)))
-        return e;
-    const long long ndraw = draw[nt];
-    const auto* T = static_cast<const IcTraj*>(dt.p);
-    const auto* D = static_cast<const long long*>(dd.p);
-    const auto* F = static_cast<const long long*>(df.p);
-    if (ndraw > 0) {
-        const int g = grid_for((ndraw + 3) / 4, 256);
-        if (f64) ic_draw_kernel<double><<<g, 256, 0, stream>>>(static_cast<double*>(states), T, D, nt, ndraw, seed, distribution);
-        else ic_draw_kernel<float><<<g, 256, 0, stream>>>(static_cast<float*>(states), T, D, nt, ndraw, seed, distribution);
+    if ((e = cudaMalloc(&dr.p, rb))) return e;
+    if ((e = cudaMemcpyAsync(dr.p, rows.data(), rb, cudaMemcpyHostToDevice, stream))) return e;
+    const auto* R = static_cast<const IcRow*>(dr.p);
+    int dev = 0, sms = 148;
+    if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+    // rows of trajectories per grid: about 16 CTAs per SM, so that a CTA takes several
+    // trajectories and the load of the next one's row overlaps the current stores
+    auto rows_for = [&](long long gx) {
+        return (unsigned)std::max(1ll, std::min<long long>({(long long)nt, 65535ll, 16ll * sms / gx}));
+    };
+    if (max_draw > 0) {
+        const long long gx = (max_draw + kIcChunk - 1) / kIcChunk;
+        const dim3 g((unsigned)gx, rows_for(gx));
+        if (f64) ic_draw_kernel<double><<<g, 256, 0, stream>>>(static_cast<double*>(states), R, nt, seed, distribution);
+        else ic_draw_kernel<float><<<g, 256, 0, stream>>>(static_cast<float*>(states), R, nt, seed, distribution);
         if ((e = cudaGetLastError())) return e;
     }
-    if (fill[nt] > 0) {
-        const int g = grid_for((fill[nt] + 7) / 8, 256);
-        if (f64) ic_fill_kernel<double><<<g, 256, 0, stream>>>(static_cast<double*>(states), T, F, nt, fill[nt], a0);
-        else ic_fill_kernel<float><<<g, 256, 0, stream>>>(static_cast<float*>(states), T, F, nt, fill[nt], (float)a0);
+    if (spin_only && max_m > 0) {
+        const long long gx = (max_m + kFillChunk - 1) / kFillChunk;
+        const dim3 g((unsigned)gx, rows_for(gx));
+        if (f64) ic_fill_kernel<double><<<g, 256, 0, stream>>>(static_cast<double*>(states), R, nt, a0);
+        else ic_fill_kernel<float><<<g, 256, 0, stream>>>(static_cast<float*>(states), R, nt, (float)a0);
         if ((e = cudaGetLastError())) return e;
     }
     return cudaStreamSynchronize(stream);
 }
 
-bool parse_cnf_body(const char* body, size_t len, long long m, std::vector<int32_t>& literals,
+bool parse_cnf_body(std::FILE* f, size_t len, long long m, std::vector<int32_t>& literals,
                     std::vector<int32_t>& lengths, std::string& msg, cudaError_t& cuda) {
     cuda = cudaSuccess;
     literals.clear();
@@ -395,7 +478,34 @@ bool parse_cnf_body(const char* body, size_t len, long long m, std::vector<int32
     AS_ING(cudaMalloc(&dhdr.p, sizeof(CnfHeader)));
     CnfHeader h{kNoFail, 0, 0, -1};
     AS_ING(cudaMemcpyAsync(dhdr.p, &h, sizeof h, cudaMemcpyHostToDevice, st));
-    if (len) AS_ING(cudaMemcpyAsync(dbody.p, body, len, cudaMemcpyHostToDevice, st));
+    {
+        // the body crosses in kStage pieces through two pinned buffers, so that reading
+        // the next piece from the file overlaps the copy of the previous one
+        constexpr size_t kStage = 4u << 20;
+        char* stage = nullptr;
+        AS_ING(cudaHostAlloc(reinterpret_cast<void**>(&stage), 2 * kStage, cudaHostAllocDefault));
+        std::unique_ptr<char, cudaError_t (*)(void*)> stage_guard(stage, cudaFreeHost);
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        AS_ING(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+        std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> ev0_guard(ev[0], cudaEventDestroy);
+        AS_ING(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+        std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> ev1_guard(ev[1], cudaEventDestroy);
+        size_t off = 0;
+        for (int i = 0; off < len; i++) {
+            const size_t c = std::min(kStage, len - off);
+            char* hbuf = stage + (i & 1) * kStage;
+            if (i >= 2) AS_ING(cudaEventSynchronize(ev[i & 1]));  // its previous copy is done
+            if (std::fread(hbuf, 1, c, f) != c) {
+                cudaStreamSynchronize(st);
+                msg = "read failed";
+                return false;
+            }
+            AS_ING(cudaMemcpyAsync(static_cast<char*>(dbody.p) + off, hbuf, c, cudaMemcpyHostToDevice, st));
+            AS_ING(cudaEventRecord(ev[i & 1], st));
+            off += c;
+        }
+        AS_ING(cudaStreamSynchronize(st));  // before the staging buffers go
+    }
     const auto* B = static_cast<const unsigned char*>(dbody.p);
     auto* H = static_cast<CnfHeader*>(dhdr.p);
     if (len) {

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -31,14 +32,15 @@ struct IcTraj {
 cudaError_t random_states(void* states, bool f64, const std::vector<IcTraj>& traj, unsigned long long seed,
                           int distribution, double a0, cudaStream_t stream);
 
-// Tokenises the clause body of a DIMACS file (the bytes after the "p cnf N M" header)
-// on the current device and returns the first m clauses: literals concatenated and
-// clause lengths (empty clauses included).  Same acceptance rules as reading the body
+// Tokenises the clause body of a DIMACS file -- the len bytes of f after the "p cnf N M"
+// header, read and copied to the current device piece by piece -- and returns the
+// first m clauses: literals concatenated and clause lengths (empty clauses included).  Same acceptance rules as reading the body
 // with fscanf("%ld") followed by a range check: returns false with msg set to
 // "expected more literals in file" or "literal out of range" on the first failure
-// in reading order, true with msg "read ok" otherwise.  cuda receives the first CUDA
-// error (then the return value is false and msg names the call).
-bool parse_cnf_body(const char* body, size_t len, long long m, std::vector<int32_t>& literals,
+// in reading order (or "read failed" when the file ends early), true with msg
+// "read ok" otherwise.  cuda receives the first CUDA error (then the return value is
+// false and msg names the call).
+bool parse_cnf_body(std::FILE* f, size_t len, long long m, std::vector<int32_t>& literals,
                     std::vector<int32_t>& lengths, std::string& msg, cudaError_t& cuda);
 
 }  // namespace asb

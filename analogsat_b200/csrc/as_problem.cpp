@@ -11,27 +11,57 @@
 namespace asb {
 
 void HostProblem::add_clauses(const int32_t* literals, const int32_t* lengths, int count) {
-    int offset = 0;
+    size_t total = 0;
+    for (int j = 0; j < count; j++) total += (size_t)std::max(lengths[j], 0);
+    storage.reserve(storage.size() + total);
+    start.reserve(start.size() + count);
+    length.reserve(length.size() + count);
+    size_t offset = 0;
+    int n_max = n, k_max = k, kept_clauses = 0;
     for (int j = 0; j < count; j++) {
         const int len = lengths[j];
         const int st = (int)storage.size();
-        int kept = 0, n_new = n;
+        int kept = 0;
         for (int i = 0; i < len; i++) {
             const int lit = literals[offset++];
             if (lit == 0) continue;
             storage.push_back(lit);
-            n_new = std::max(n_new, std::abs(lit));
+            n_max = std::max(n_max, std::abs(lit));
             kept++;
         }
         if (kept == 0) continue;  // empty clauses are dropped (SatProblem.cpp:52)
         start.push_back(st);
         length.push_back(kept);
-        k = std::max(k, kept);
-        n = n_new;
-        m++;
+        k_max = std::max(k_max, kept);
+        kept_clauses++;
     }
+    n = n_max;
+    k = k_max;
+    m += kept_clauses;
 }
 
+void HostProblem::set_clauses(std::vector<int32_t>&& literals, const std::vector<int32_t>& lengths) {
+    *this = HostProblem();
+    storage = std::move(literals);
+    start.reserve(lengths.size());
+    length.reserve(lengths.size());
+    int32_t off = 0;
+    for (const int32_t len : lengths) {
+        if (len > 0) {  // empty clauses are dropped (SatProblem.cpp:84)
+            start.push_back(off);
+            length.push_back(len);
+            k = std::max(k, (int)len);
+            m++;
+        }
+        off += len;
+    }
+    int nmax = 0;
+    for (const int32_t v : storage) nmax = std::max(nmax, v < 0 ? -v : v);
+    n = nmax;
+}
+
+// Lines before the declaration are skipped whole (CnfReader.cpp:61-82); an empty line
+// is skipped on its own rather than taking the next line with it.
 bool read_cnf_header(std::FILE* f, int& n, int& m, std::string& msg) {
     n = -1;
     m = -1;

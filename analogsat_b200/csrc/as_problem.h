@@ -59,6 +59,9 @@ struct HostProblem {
 
     // SatProblem::AddClauses(literals, lengths) (SatProblem.cpp:64-95)
     void add_clauses(const int32_t* literals, const int32_t* lengths, int count);
+    // The same on an empty problem for zero-free literals (a tokenised CNF body), taking
+    // over the literal array instead of copying it.
+    void set_clauses(std::vector<int32_t>&& literals, const std::vector<int32_t>& lengths);
 };
 
 // CnfReader::Read (AnalogSAT/io/CnfReader.cpp:48-141).  Returns false and fills msg on error.
