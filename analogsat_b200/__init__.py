@@ -368,10 +368,15 @@ class SatSolver:
                                               solver_name.encode()))
 
     def GetSatState(self, traj: int = 0, dtype=np.float64) -> np.ndarray:
-        allst = self.GetSatStates(dtype)
-        off = int(sum(sum(self._nm[p]) for p in self._traj_problem[:traj]))
+        """Final public state of one trajectory (one device-to-host copy)."""
+        if not 0 <= traj < len(self._traj_problem):
+            raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "trajectory index out of range")
         n, m = self._nm[self._traj_problem[traj]]
-        return allst[off: off + n + m]
+        out = np.zeros(n + m, dtype)
+        fn = (self._lib.as_solver_get_state_f32 if out.dtype == np.float32
+              else self._lib.as_solver_get_state_f64)
+        check(fn(self._h, int(traj), out.ctypes.data_as(C.c_void_p)))
+        return out
 
     def GetBestAssignment(self, traj: int) -> np.ndarray:
         n, _ = self._nm[self._traj_problem[traj]]

@@ -72,6 +72,8 @@ SIGNATURES = [
     ("as_solver_get_results", _i32, [_vp, _pi32, _pf64, _pi32, _pi32, _pi32, _pi32, _pi32, _pf64]),
     ("as_solver_get_states_f64", _i32, [_vp, _vp]),
     ("as_solver_get_states_f32", _i32, [_vp, _vp]),
+    ("as_solver_get_state_f64", _i32, [_vp, _i32, _vp]),
+    ("as_solver_get_state_f32", _i32, [_vp, _i32, _vp]),
     ("as_solver_states_device", _vp, [_vp]),
     ("as_solver_get_best_assignment", _i32, [_vp, _i32, _vp]),
     ("as_solver_get_launch_shape", _i32, [_vp, _pi32, _pi32, _pi32, _pi32]),

@@ -724,6 +724,11 @@ int plan_units(as_solver* s, const int32_t* problem_index, int num_traj) {
     for (int t = 0; t < num_traj; t++)
         if (problem_index[t] < 0 || problem_index[t] >= np)
             return fail(AS_ERR_BAD_INPUT, "problem index out of range");
+    // the same trajectories as the last call: buffers, unit tables and the captured
+    // solve stay valid, only the state values change
+    if (num_traj == s->num_traj && s->states.p &&
+        std::equal(problem_index, problem_index + num_traj, s->traj_problem.begin()))
+        return AS_OK;
     s->num_traj = num_traj;
     s->traj_problem.assign(problem_index, problem_index + num_traj);
     s->traj_off.resize(num_traj);
@@ -798,11 +803,19 @@ int build_groups(as_solver* s) {
         }
     }
     const auto& pi = s->traj_problem;
+    // Within a launch shape the work queue deals the problems round-robin (the r-th
+    // trajectory of every problem before the (r+1)-th of any), so the trajectories
+    // running at once belong to different problems: with stop-on-first an instance's
+    // restarts then run a few at a time instead of filling the GPU together and being
+    // stopped together.
+    std::vector<int> rank(num_traj), seen(np, 0);
+    for (int t = 0; t < num_traj; t++) rank[t] = seen[pi[t]]++;
     s->order.resize(num_traj);
     for (int t = 0; t < num_traj; t++) s->order[t] = t;
     std::stable_sort(s->order.begin(), s->order.end(), [&](int a, int b) {
         const int va = pv[pi[a]], vb = pv[pi[b]];
         if (va != vb) return va < vb;
+        if (rank[a] != rank[b]) return rank[a] < rank[b];
         return pi[a] < pi[b];
     });
     s->groups.clear();
@@ -1482,7 +1495,35 @@ int get_states(as_solver* s, DST* out) {
 }
 }  // namespace
 
+template <typename DST>
+int get_state_one(as_solver* s, int32_t traj, DST* out) {
+    if (!s || !out) return fail(AS_ERR_BAD_INPUT, "as_solver_get_state: null argument");
+    if (traj < 0 || traj >= s->num_traj) return fail(AS_ERR_BAD_INPUT, "trajectory index out of range");
+    AS_CUDA(cudaSetDevice(s->device));
+    const auto& q = s->problems[s->traj_problem[traj]];
+    const size_t n = (size_t)q.n + q.m;
+    const size_t vb = s->precision == AS_PREC_F64 ? 8 : 4;
+    const char* src = static_cast<const char*>(s->states.p) + (size_t)s->traj_off[traj] * vb;
+    if (vb == sizeof(DST)) {
+        AS_CUDA(cudaMemcpyAsync(out, src, n * vb, cudaMemcpyDeviceToHost, s->stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+    } else if (vb == 8) {
+        std::vector<double> tmp(n);
+        AS_CUDA(cudaMemcpyAsync(tmp.data(), src, n * 8, cudaMemcpyDeviceToHost, s->stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+        for (size_t i = 0; i < n; i++) out[i] = (DST)tmp[i];
+    } else {
+        std::vector<float> tmp(n);
+        AS_CUDA(cudaMemcpyAsync(tmp.data(), src, n * 4, cudaMemcpyDeviceToHost, s->stream));
+        AS_CUDA(cudaStreamSynchronize(s->stream));
+        for (size_t i = 0; i < n; i++) out[i] = (DST)tmp[i];
+    }
+    return AS_OK;
+}
+
 int32_t as_solver_get_states_f64(as_solver* s, double* out) { return get_states<double>(s, out); }
+int32_t as_solver_get_state_f64(as_solver* s, int32_t traj, double* out) { return get_state_one<double>(s, traj, out); }
+int32_t as_solver_get_state_f32(as_solver* s, int32_t traj, float* out) { return get_state_one<float>(s, traj, out); }
 int32_t as_solver_get_states_f32(as_solver* s, float* out) { return get_states<float>(s, out); }
 const void* as_solver_states_device(as_solver* s) { return s ? s->states.p : nullptr; }
 

@@ -254,6 +254,19 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         const int u = g.bcast(&s_unit, tid == 0 ? atomicAdd(P.queue_head, 1) : 0);
         if (u >= P.num_units) break;
         const int pidx = P.unit_inst[u];
+        // an instance already solved by another trajectory (stop_on_first) is skipped,
+        // its state left as it was set
+        if (g.bcast(&s_flag, tid == 0 && P.stop_on_first ? (atomicAdd(P.inst_solved + pidx, 0) != 0 ? 1 : 0) : 0)) {
+            if (tid == 0) {
+                UnitResult r;
+                r.time = 0.0; r.hdid = 0.0; r.status = SAT_ODE_INTERRUPTED; r.steps = 0; r.attempts = 0;
+                r.rhs = 0; r.viol = -1; r.min_viol = -1;
+                r.pad0 = r.pad1 = 0;
+                P.results[u] = r;
+            }
+            g.sync();  // s_unit / s_flag are reused by the next unit
+            continue;
+        }
         const DevInstance I = P.inst[pidx];
         const int n = I.n, E = I.n + I.m;
         const int Ep = (E + 3) & ~3;
@@ -279,10 +292,6 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         double t = 0.0, hnext = 1e-9, hdid = 0.0;
         int steps = 0, attempts = 0, rhs = 0, viol = -1, minviol = INT_MAX;
         int status = SAT_UNKNOWN;
-
-        // an instance already solved by another trajectory (stop_on_first) is skipped
-        const int skip = g.bcast(&s_flag, tid == 0 && P.stop_on_first ? (atomicAdd(P.inst_solved + pidx, 0) != 0 ? 1 : 0) : 0);
-        if (skip) status = SAT_ODE_INTERRUPTED;
 
         while (status == SAT_UNKNOWN && t < P.tmax && steps < P.maxsteps) {
             bool underflow = false, interrupted = false;

@@ -52,7 +52,7 @@ WORKLOAD = dict(name="planted-3sat-N1000-M4250-x64-inst-x256-traj", instances=64
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--instances", type=int, default=WORKLOAD["instances"])
@@ -202,8 +202,10 @@ def run_reference(args):
     vals, rhs = [], []
     for i in range(args.warmup):
         cpu_baseline(probs, pidx, ics, 2.0)
+    # a bounded sample per step, so that the whole run stays near a minute and a half
+    per_step = max(3.0, min(args.cpu_sample_seconds, 90.0 / max(args.steps, 1)))
     for i in range(args.steps):
-        c = cpu_baseline(probs, pidx, ics, args.cpu_sample_seconds)
+        c = cpu_baseline(probs, pidx, ics, per_step)
         vals.append(c)
     v = float(np.mean([c["value"] for c in vals]))
     wall = float(np.sum([c["wall"] for c in vals]))
@@ -219,7 +221,7 @@ def run_reference(args):
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": vals[0]["threads"],
                          "kind": "reference",
                          "sample": f"first trajectories (round-robin over instances) of the "
-                                   f"workload, {args.cpu_sample_seconds:.0f} s of wall per step, "
+                                   f"workload, {per_step:.0f} s of wall per step, "
                                    f"reference CpuSat<double>+CpuRungeKutta<double> via SatSolver, "
                                    f"{vals[0]['threads']} threads on {cpu_name()}"},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -304,25 +306,29 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         host_in = torch.from_numpy(ics).pin_memory().numpy()
-        host_out = torch.empty(ics.size, dtype=torch.float32).pin_memory().numpy()
         solver.SetSatStates(pidx, host_in)
         solver.Solve()
         barrier()
         t0 = time.perf_counter()
         e_solved = 0
+        d2h = 0
         for _ in range(args.steps):
             solver.SetSatStates(pidx, host_in)
             solver.Solve()
+            # the step's result: every trajectory's SatResult and counters, and the
+            # final state (the satisfying assignment) of every solved trajectory
             r = solver.results()
-            solver.GetSatStates(np.float32, out=host_out)
-            e_solved += (int((r["status"] == 0).sum()) if args.all_trajectories
-                         else len(set(pidx[r["status"] == 0])))
+            won = np.nonzero(r["status"] == 0)[0]
+            for u in won:
+                solver.GetSatState(int(u), np.float32)
+            d2h += len(pidx) * 48 + 4 * nm * len(won)
+            e_solved += (len(won) if args.all_trajectories else len(set(pidx[won])))
         barrier()
         t_e = time.perf_counter() - t0
         (e_solved,), t_e = reduce_over_ranks(dist, [e_solved], t_e, "cuda")
-        res_bytes = len(pidx) * 48
         e2e = {"value": e_solved / t_e, "unit": "solves/s", "h2d_bytes_per_step": int(ics.nbytes),
-               "d2h_bytes_per_step": int(ics.nbytes + res_bytes), "seconds": t_e}
+               "d2h_bytes_per_step": int(d2h // args.steps), "seconds": t_e,
+               "result_read": "SatResult and counters of every trajectory + final state of each solved one"}
 
     if rank != 0:
         if dist is not None:

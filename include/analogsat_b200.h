@@ -217,6 +217,9 @@ int32_t as_solver_get_results(as_solver* s, int32_t* status, double* time, int32
  * trajectories, concatenated as in as_solver_set_states_*. */
 int32_t as_solver_get_states_f64(as_solver* s, double* states);
 int32_t as_solver_get_states_f32(as_solver* s, float* states);
+/* The same for one trajectory: its N + M public values, one device-to-host copy. */
+int32_t as_solver_get_state_f64(as_solver* s, int32_t traj, double* state);
+int32_t as_solver_get_state_f32(as_solver* s, int32_t traj, float* state);
 /* Device pointer of the solver's state buffer (solver precision), for zero-copy reads. */
 const void* as_solver_states_device(as_solver* s);
 

@@ -255,14 +255,13 @@ public:
     }
 
     std::vector<TFloat> GetSatState(int traj) const {
-        std::vector<TFloat> all(total());
+        if (traj < 0 || traj >= (int)index_.size()) throw Error(AS_ERR_BAD_INPUT, "trajectory index out of range");
+        std::vector<TFloat> x(nm_[index_[traj]]);
         if (kPrecision == AS_PREC_F64)
-            check(as_solver_get_states_f64(s_.get(), reinterpret_cast<double*>(all.data())));
+            check(as_solver_get_state_f64(s_.get(), traj, reinterpret_cast<double*>(x.data())));
         else
-            check(as_solver_get_states_f32(s_.get(), reinterpret_cast<float*>(all.data())));
-        size_t off = 0;
-        for (int t = 0; t < traj; t++) off += nm_[index_[t]];
-        return std::vector<TFloat>(all.begin() + off, all.begin() + off + nm_[index_[traj]]);
+            check(as_solver_get_state_f32(s_.get(), traj, reinterpret_cast<float*>(x.data())));
+        return x;
     }
 
     int GetStepCount(int traj) const { return steps_.at(traj); }
