@@ -61,6 +61,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-rhs-bench", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shape instead of the autotuned one")
     ap.add_argument("--all-trajectories", action="store_true",
                     help="run every trajectory to its own SatResult (no early exit per instance)")
     ap.add_argument("--workload", default="planted1000",
@@ -252,6 +254,15 @@ def run_ours(args):
     solver.SetMaxSteps(args.max_steps)
     solver.SetMaxTime(W["tmax"])
     solver.SetStopOnFirst(not args.all_trajectories)
+    shape = None
+    if not args.no_autotune:
+        # launch shape (CTA size, storage mode) picked by timing fixed-work solves of
+        # this instance size, outside the timed region (analogsat_b200/autotune.py)
+        from analogsat_b200 import autotune
+        best = autotune.tune(probs[0], A.AS_PREC_F32_LOGA, save=False)
+        shape = {"threads": best["threads"], "storage": best["storage"]}
+        solver.ForceThreads(shape["threads"])
+        solver.SetStorageMode(shape["storage"])
     ics_dev = torch.from_numpy(ics).cuda()
     st = torch.cuda.Stream()
     nm = W["n"] + W["m"]
@@ -313,6 +324,9 @@ def run_ours(args):
         other = pair[1]
         other.SetEpsilon(W["eps"]); other.SetBatchSize(W["batch"]); other.SetMaxSteps(args.max_steps)
         other.SetMaxTime(W["tmax"]); other.SetStopOnFirst(not args.all_trajectories)
+        if shape:
+            other.ForceThreads(shape["threads"])
+            other.SetStorageMode(shape["storage"])
 
         def issue(s):
             s.SetSatStates(pidx, host_in)  # asynchronous from pinned memory
@@ -382,6 +396,7 @@ def run_ours(args):
         "mode": "all trajectories to their own result" if args.all_trajectories
         else "first solution per instance stops its other trajectories",
         "gpu_launches": args.steps * len(solver_groups(solver)),
+        "launch_shape": dict(solver.launch_shape(), autotuned=shape is not None),
         "roofline": {"bound": "hbm", "kernel": "solve_kernel", "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      # ncu dram__bytes_read+write of one solve_kernel launch over 148
