@@ -172,3 +172,21 @@ def test_stream_wall_budget():
     assert (r["status"] == 2).all()
     assert wall < 10.0
     assert (r["steps"] > 0).all()
+
+
+def test_stream_f32_error_at_maxsat_size(oracle):
+    """The MAXSAT configuration's size (random 4-SAT N=1e5, M=1e6): an FP32 streamed
+    trajectory after 40 accepted steps against the FP64 oracle's solution of the same
+    ODE at the same time (eps 1e-10), <= 1e-5 relative to max(|x|, 1)."""
+    from analogsat_b200 import SatProblem
+    from analogsat_b200.instances import make_instance, initial_states
+    n, m = 100_000, 1_000_000
+    lits, lens, _ = make_instance("fast", n, m, 4, seed=5000)
+    p = SatProblem.from_arrays(lits, lens)
+    ics = initial_states(n, m, 1, seed=3, dtype=np.float32)
+    r, X = _run([p], 0, np.zeros(1), ics, 3, batch=10, maxsteps=40)
+    assert r["steps"][0] == 40
+    o = oracle.integrate_to(oracle.problem(lits, lens), ics[0].astype(np.float64), r["time"][0], eps=1e-10)
+    err = np.abs(X.astype(np.float64) - o["state"]) / np.maximum(np.abs(o["state"]), 1.0)
+    print(f"N=1e5/M=1e6 FP32 stream vs FP64 oracle at t={r['time'][0]:.4g}: max rel err {err.max():.3g}")
+    assert err.max() <= 1e-5, err.max()
