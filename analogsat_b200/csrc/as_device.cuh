@@ -140,7 +140,10 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
         if (EXACT || q < I.k) {
             w[q].load(I, q * I.mp + m);
             const T s = sy[w[q].var()];
-            f[q] = w[q].neg() ? A::add(T(1), s) : A::sub(T(1), s);
+            if constexpr (sizeof(T) == 4)  // 1 - (-s) == 1 + s: the literal's sign bit flips s
+                f[q] = T(1) - __int_as_float(__float_as_int(s) ^ (int)(w[q].w & 0x80000000u));
+            else
+                f[q] = w[q].neg() ? A::add(T(1), s) : A::sub(T(1), s);
             km = A::mul(km, f[q]);
         }
     }
@@ -200,9 +203,14 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
                         first = false;
                     }
                 }
-                T rr = A::mul(r, prod);
-                rr = rr + rr;
-                cs[w[q].slot()] = w[q].neg() ? -rr : rr;
+                if constexpr (sizeof(T) == 4) {  // (2r) prod == 2 (r prod) above the subnormals
+                    const T rr = (r + r) * prod;
+                    cs[w[q].slot()] = __int_as_float(__float_as_int(rr) ^ (int)(w[q].w & 0x80000000u));
+                } else {
+                    T rr = A::mul(r, prod);
+                    rr = rr + rr;
+                    cs[w[q].slot()] = w[q].neg() ? -rr : rr;
+                }
             }
         }
     } else {
