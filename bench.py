@@ -63,6 +63,8 @@ def parse_args():
     ap.add_argument("--no-rhs-bench", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shape instead of the autotuned one")
+    ap.add_argument("--threads", type=int, default=0,
+                    help="force this CTA size for the solver (no autotuning)")
     ap.add_argument("--all-trajectories", action="store_true",
                     help="run every trajectory to its own SatResult (no early exit per instance)")
     ap.add_argument("--workload", default="planted1000",
@@ -255,7 +257,10 @@ def run_ours(args):
     solver.SetMaxTime(W["tmax"])
     solver.SetStopOnFirst(not args.all_trajectories)
     shape = None
-    if not args.no_autotune:
+    if args.threads:
+        shape = {"threads": args.threads, "storage": 0}
+        solver.ForceThreads(args.threads)
+    elif not args.no_autotune:
         # launch shape (CTA size, storage mode) picked by timing fixed-work solves of
         # this instance size, outside the timed region (analogsat_b200/autotune.py)
         from analogsat_b200 import autotune
@@ -396,7 +401,7 @@ def run_ours(args):
         "mode": "all trajectories to their own result" if args.all_trajectories
         else "first solution per instance stops its other trajectories",
         "gpu_launches": args.steps * len(solver_groups(solver)),
-        "launch_shape": dict(solver.launch_shape(), autotuned=shape is not None),
+        "launch_shape": dict(solver.launch_shape(), autotuned=shape is not None and not args.threads),
         "roofline": {"bound": "hbm", "kernel": "solve_kernel", "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                      # ncu dram__bytes_read+write of one solve_kernel launch over 148
