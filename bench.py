@@ -206,8 +206,9 @@ def run_reference(args):
     vals, rhs = [], []
     for i in range(args.warmup):
         cpu_baseline(probs, pidx, ics, 2.0)
-    # a bounded sample per step, so that the whole run stays near a minute and a half
-    per_step = max(3.0, min(args.cpu_sample_seconds, 90.0 / max(args.steps, 1)))
+    # a bounded sample per step (new trajectories stop at per_step seconds, running ones
+    # at twice that), so that the whole run stays within about two minutes
+    per_step = max(2.0, min(args.cpu_sample_seconds, 60.0 / max(args.steps, 1)))
     for i in range(args.steps):
         c = cpu_baseline(probs, pidx, ics, per_step)
         vals.append(c)

@@ -154,7 +154,8 @@ int steps_impl(void* handle, const T* ic, T eps, int nsteps, double* times, doub
 
 template <typename T>
 int solve_impl(void* handle, const T* ic, T eps, T tmax, int maxsteps, int batch, T* final_state,
-               double* out_time, int* out_steps, int* out_rhs, int* out_viol, double* out_wall) {
+               double* out_time, int* out_steps, int* out_rhs, int* out_viol, double* out_wall,
+               const std::chrono::steady_clock::time_point* deadline = nullptr) {
     try {
         const SatProblem& p = *static_cast<SatProblem*>(handle);
         const int nm = p.Get_N() + p.Get_M();
@@ -162,6 +163,10 @@ int solve_impl(void* handle, const T* ic, T eps, T tmax, int maxsteps, int batch
         rs.solver.SetMaxTime(tmax);
         rs.solver.SetMaxSteps(maxsteps);
         rs.solver.SetBatchSize(batch);
+        if (deadline) {  // the reference's own per-batch callback stops the run (SAT_ODE_INTERRUPTED)
+            const auto d = *deadline;
+            rs.solver.SetCallback([d](SatSolver<T, CpuODEState<T>>&) { return std::chrono::steady_clock::now() < d; });
+        }
         std::vector<T> v(ic, ic + nm);
         rs.solver.SetSatState(v);
         SatResult r = rs.solver.Solve();
@@ -290,8 +295,10 @@ int ref_solve_f(void* h, const float* ic, float eps, float tmax, int maxsteps, i
 // Many independent FP64 solves spread over `nthreads` host threads (the reference
 // solver is single-threaded; every thread owns its own CpuSatSolver).  Unit u
 // solves problems[prob_idx[u]] from ics[ic_off[u] ...].  Threads stop taking new
-// units once `wall_budget` seconds have passed; done[u] = 1 marks units run.
-// Returns the number of units completed and the elapsed wall seconds in *wall.
+// units once `wall_budget` seconds have passed, and a unit still running at twice
+// the budget is interrupted through the solver's callback and left out (done[u] = 0);
+// done[u] = 1 marks units run to their own result.  Returns the number of units
+// completed and the elapsed wall seconds in *wall.
 int ref_solve_many_d(void** problems, const int* prob_idx, const double* ics,
                      const long long* ic_off, int nunits, int nthreads, double eps, double tmax,
                      int maxsteps, int batch, double wall_budget, int* results, int* steps,
@@ -299,6 +306,8 @@ int ref_solve_many_d(void** problems, const int* prob_idx, const double* ics,
     std::atomic<int> next(0);
     std::atomic<int> completed(0);
     auto t0 = std::chrono::steady_clock::now();
+    const auto hard = t0 + std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                               std::chrono::duration<double>(2.0 * wall_budget));
     auto worker = [&]() {
         while (true) {
             double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -306,8 +315,11 @@ int ref_solve_many_d(void** problems, const int* prob_idx, const double* ics,
             int u = next.fetch_add(1);
             if (u >= nunits) break;
             double tm = 0; int st = 0, rc = 0, vi = 0; double w = 0;
-            results[u] = solve_impl<double>(problems[prob_idx[u]], ics + ic_off[u], eps, tmax,
-                                            maxsteps, batch, nullptr, &tm, &st, &rc, &vi, &w);
+            const int r = solve_impl<double>(problems[prob_idx[u]], ics + ic_off[u], eps, tmax, maxsteps,
+                                             batch, nullptr, &tm, &st, &rc, &vi, &w,
+                                             wall_budget > 0 ? &hard : nullptr);
+            if (wall_budget > 0 && r == SAT_ODE_INTERRUPTED) continue;  // cut at the hard deadline
+            results[u] = r;
             steps[u] = st; rhs[u] = rc; times[u] = tm; done[u] = 1;
             completed.fetch_add(1);
         }
