@@ -214,7 +214,7 @@ class Reference:
         L.ref_solve_many_d.restype = C.c_int
         L.ref_solve_many_d.argtypes = [C.POINTER(C.c_void_p), _i32p, _f64p, _i64p, C.c_int,
                                        C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
-                                       C.c_double, _i32p, _i32p, _i32p, _f64p, _i32p,
+                                       C.c_double, _i32p, _i32p, _i32p, _f64p, _i32p, _f64p,
                                        C.POINTER(C.c_double)]
         L.ref_minisat.restype = C.c_int
         L.ref_minisat.argtypes = [C.c_void_p, C.c_void_p]
@@ -318,12 +318,12 @@ class Reference:
         if n > 1:
             offs[1:] = np.cumsum([len(x) for x in ics])[:-1]
         res = np.full(n, -1, np.int32); st = np.zeros(n, np.int32); rh = np.zeros(n, np.int32)
-        tm = np.zeros(n); done = np.zeros(n, np.int32); wall = C.c_double()
+        tm = np.zeros(n); done = np.zeros(n, np.int32); busy = np.zeros(n); wall = C.c_double()
         comp = self.L.ref_solve_many_d(handles, prob_idx, flat, offs, n, nthreads, eps, tmax,
-                                       maxsteps, batch, wall_budget, res, st, rh, tm, done,
+                                       maxsteps, batch, wall_budget, res, st, rh, tm, done, busy,
                                        C.byref(wall))
         return dict(completed=comp, result=res, steps=st, rhs=rh, time=tm, done=done,
-                    wall=wall.value, threads=nthreads)
+                    busy=busy, wall=wall.value, threads=nthreads)
 
     def minisat(self, p):
         sol = np.zeros(max(p.n, 1), np.int32)

@@ -297,12 +297,12 @@ int ref_solve_f(void* h, const float* ic, float eps, float tmax, int maxsteps, i
 // solves problems[prob_idx[u]] from ics[ic_off[u] ...].  Threads stop taking new
 // units once `wall_budget` seconds have passed, and a unit still running at twice
 // the budget is interrupted through the solver's callback and left out (done[u] = 0);
-// done[u] = 1 marks units run to their own result.  Returns the number of units
-// completed and the elapsed wall seconds in *wall.
+// done[u] = 1 marks units run to their own result, busy[u] their wall seconds.
+// Returns the number of units completed and the elapsed wall seconds in *wall.
 int ref_solve_many_d(void** problems, const int* prob_idx, const double* ics,
                      const long long* ic_off, int nunits, int nthreads, double eps, double tmax,
                      int maxsteps, int batch, double wall_budget, int* results, int* steps,
-                     int* rhs, double* times, int* done, double* wall) {
+                     int* rhs, double* times, int* done, double* busy, double* wall) {
     std::atomic<int> next(0);
     std::atomic<int> completed(0);
     auto t0 = std::chrono::steady_clock::now();
@@ -315,10 +315,12 @@ int ref_solve_many_d(void** problems, const int* prob_idx, const double* ics,
             int u = next.fetch_add(1);
             if (u >= nunits) break;
             double tm = 0; int st = 0, rc = 0, vi = 0; double w = 0;
+            const auto u0 = std::chrono::steady_clock::now();
             const int r = solve_impl<double>(problems[prob_idx[u]], ics + ic_off[u], eps, tmax, maxsteps,
                                              batch, nullptr, &tm, &st, &rc, &vi, &w,
                                              wall_budget > 0 ? &hard : nullptr);
             if (wall_budget > 0 && r == SAT_ODE_INTERRUPTED) continue;  // cut at the hard deadline
+            if (busy) busy[u] = std::chrono::duration<double>(std::chrono::steady_clock::now() - u0).count();
             results[u] = r;
             steps[u] = st; rhs[u] = rc; times[u] = tm; done[u] = 1;
             completed.fetch_add(1);
