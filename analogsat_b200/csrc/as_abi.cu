@@ -835,7 +835,15 @@ int build_groups(as_solver* s) {
         G.variant = vi;
         G.u0 = u;
         G.u1 = e;
-        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : 512) : bt);
+        // global storage: 512 threads (two CTAs per SM) while the in-flight slabs fit in
+        // L2, else 1,024 (one per SM, half the slabs)
+        int gs_bt = 512;
+        if (v.gs && v.cl == 1) {
+            int l2 = 0;
+            AS_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->device));
+            if (2.0 * s->sm_count * (double)vals * v.bytes_per_value > 0.75 * l2) gs_bt = 1024;
+        }
+        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : gs_bt) : bt);
         G.smem = v.gs ? 0 : vals * v.bytes_per_value;
         AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem));
         int occ = 0;
