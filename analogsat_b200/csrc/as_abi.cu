@@ -843,7 +843,15 @@ int build_groups(as_solver* s) {
             AS_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->device));
             if (2.0 * s->sm_count * (double)vals * v.bytes_per_value > 0.75 * l2) gs_bt = 1024;
         }
-        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : gs_bt) : bt);
+        // shared memory: a trajectory that leaves no room for a second CTA on the SM gets
+        // the largest CTA (more warps to hide the clause phase's latencies)
+        int sm_bt = bt;
+        if (!v.gs) {
+            int per_sm = 0;
+            AS_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, s->device));
+            if (2 * (vals * v.bytes_per_value + 2048) > (size_t)per_sm) sm_bt = 1024;
+        }
+        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : gs_bt) : sm_bt);
         G.smem = v.gs ? 0 : vals * v.bytes_per_value;
         AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem));
         int occ = 0;
