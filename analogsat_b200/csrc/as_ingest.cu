@@ -223,33 +223,48 @@ __device__ void scan_long(const unsigned char* __restrict__ body, long long len,
     }
 }
 
-// Scans one thread's 16 bytes at body position p0 (own: those bytes, next: the 16
-// after them, prev: the byte before).  For each literal starting here calls
-// emit(position, value, negative, zero) (value only when VALUES); returns the packed counts tokens << 16 |
-// zeros and lowers fail to the first failure among these bytes.
-template <bool VALUES, typename F>
-__device__ __forceinline__ int scan_bytes(const unsigned char* __restrict__ body, long long len, long long p0,
-                                          const uint4& own, const uint4& next, int prev, unsigned long long& fail,
-                                          F&& emit) {
+// Byte-class masks of one thread's 16 bytes at body position p0 (own: those bytes,
+// next: the 16 after them, prev: the byte before): bit i of dig / nz is byte i of the
+// 32 (digit / digit 1-9), of mn and starts byte i of the own 16 ('-' / first digit of
+// a literal).  Lowers fail to the first malformed byte among the own 16.
+struct ByteMasks {
+    unsigned dig, nz, mn, starts;
+    bool prev_mn;
+};
+
+__device__ __forceinline__ ByteMasks byte_masks(long long len, long long p0, const uint4& own, const uint4& next,
+                                                int prev, unsigned long long& fail) {
+    ByteMasks k{0u, 0u, 0u, 0u, false};
     const long long avail = len - p0;
-    if (avail <= 0) return 0;
+    if (avail <= 0) return k;
     const unsigned valid = avail >= 32 ? 0xffffffffu : (1u << avail) - 1u;
-    const unsigned dig = (mask16<cls_digit>(own) | mask16<cls_digit>(next) << 16) & valid;
-    const unsigned nz = (mask16<cls_nonzero>(own) | mask16<cls_nonzero>(next) << 16) & valid;
+    k.dig = (mask16<cls_digit>(own) | mask16<cls_digit>(next) << 16) & valid;
+    k.nz = (mask16<cls_nonzero>(own) | mask16<cls_nonzero>(next) << 16) & valid;
     const unsigned sp = mask16<cls_space>(own) & valid;
     const unsigned sg = mask16<cls_sign>(own) & valid;
-    const unsigned mn = mask16<cls_minus>(own) & valid;
+    k.mn = mask16<cls_minus>(own) & valid;
     const unsigned prev_dig = (prev >= '0' && prev <= '9') ? 1u : 0u;
-    const unsigned prev_mn = prev == '-' ? 1u : 0u;
+    k.prev_mn = prev == '-';
     // failures: a byte of no class, a sign without a digit right after it
-    const unsigned bad = ((~(dig | sp | sg) & valid) | (sg & ~(dig >> 1))) & 0xffffu;
+    const unsigned bad = ((~(k.dig | sp | sg) & valid) | (sg & ~(k.dig >> 1))) & 0xffffu;
     if (bad) fail = min(fail, (unsigned long long)(p0 + __ffs(bad) - 1) << 1);
-    unsigned starts = dig & ~((dig << 1) | prev_dig) & 0xffffu;
+    k.starts = k.dig & ~((k.dig << 1) | prev_dig) & 0xffffu;
+    return k;
+}
+
+// Walks the literals starting in these 16 bytes: emit(position, value, negative,
+// zero) for each (value only when VALUES); returns the packed counts tokens << 16 |
+// zeros and lowers fail at an out-of-range literal.
+template <bool VALUES, typename F>
+__device__ __forceinline__ int walk_literals(const unsigned char* __restrict__ body, long long len, long long p0,
+                                             const uint4& own, const uint4& next, const ByteMasks& k,
+                                             unsigned long long& fail, F&& emit) {
+    unsigned starts = k.starts;
     int tok = 0, zero = 0;
     while (starts) {
         const int s = __ffs(starts) - 1;
         starts &= starts - 1;
-        const unsigned rest = ~(dig >> s);  // bit j: byte s + j is not a digit
+        const unsigned rest = ~(k.dig >> s);  // bit j: byte s + j is not a digit
         const int e = rest ? s + __ffs(rest) - 1 : 32;
         long long v = 0;
         bool range = false, is_zero;
@@ -258,7 +273,7 @@ __device__ __forceinline__ int scan_bytes(const unsigned char* __restrict__ body
             is_zero = v == 0;
         } else {
             const unsigned run = (1u << (e - s)) - 1u;
-            const unsigned nzr = (nz >> s) & run;
+            const unsigned nzr = (k.nz >> s) & run;
             is_zero = nzr == 0;
             if (!is_zero) {
                 const int sig = e - s - (__ffs(nzr) - 1);  // digits after the leading zeros
@@ -271,7 +286,7 @@ __device__ __forceinline__ int scan_bytes(const unsigned char* __restrict__ body
             }
         }
         if (range) fail = min(fail, ((unsigned long long)(p0 + s) << 1) | 1ull);
-        const bool neg = s ? ((mn >> (s - 1)) & 1u) : prev_mn;
+        const bool neg = s ? ((k.mn >> (s - 1)) & 1u) : k.prev_mn;
         emit(p0 + s, range ? 0 : (int)v, neg, is_zero);
         tok++;
         zero += is_zero;
@@ -297,8 +312,9 @@ __global__ void __launch_bounds__(kCnfThreads) cnf_count_kernel(const unsigned c
     const uint4 own = *reinterpret_cast<const uint4*>(sb + 16 + kCnfBytes * tid);
     const uint4 next = *reinterpret_cast<const uint4*>(sb + 32 + kCnfBytes * tid);
     unsigned long long fail = kNoFail;
-    int c = scan_bytes<false>(body, len, base + (long long)kCnfBytes * tid, own, next, sb[15 + kCnfBytes * tid], fail,
-                       [](long long, int, bool, bool) {});
+    const long long p0 = base + (long long)kCnfBytes * tid;
+    const ByteMasks k = byte_masks(len, p0, own, next, sb[15 + kCnfBytes * tid], fail);
+    int c = walk_literals<false>(body, len, p0, own, next, k, fail, [](long long, int, bool, bool) {});
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
     fail = warp_min64(fail);
@@ -375,7 +391,8 @@ __global__ void __launch_bounds__(kCnfThreads) cnf_emit_kernel(const unsigned ch
     const int prev = sb[15 + kCnfBytes * tid];
     const long long p0 = base + (long long)kCnfBytes * tid;
     unsigned long long fail = kNoFail;
-    const int c = scan_bytes<false>(body, len, p0, own, next, prev, fail, [](long long, int, bool, bool) {});
+    const ByteMasks bm = byte_masks(len, p0, own, next, prev, fail);
+    const int c = walk_literals<false>(body, len, p0, own, next, bm, fail, [](long long, int, bool, bool) {});
     // exclusive block scan of the packed counts
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int inc = c;
@@ -391,7 +408,7 @@ __global__ void __launch_bounds__(kCnfThreads) cnf_emit_kernel(const unsigned ch
     const int ex = before + inc - c;
     long long k = tok_pre[blockIdx.x] + (ex >> 16);
     long long z = zero_pre[blockIdx.x] + (ex & 0xffff);
-    scan_bytes<true>(body, len, p0, own, next, prev, fail, [&](long long q, int v, bool neg, bool is_zero) {
+    walk_literals<true>(body, len, p0, own, next, bm, fail, [&](long long q, int v, bool neg, bool is_zero) {
         if (z < m) {
             if (is_zero) {
                 ends[z] = (int)(k - z);
