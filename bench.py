@@ -122,6 +122,7 @@ class Clocks:
         self.p = None
 
     def __enter__(self):
+        self.skip = 0
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
@@ -129,10 +130,29 @@ class Clocks:
                 stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return self
+        # wait until the sampler runs, so that the samples kept are the timed region's
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.p.poll() is None:
+            self.f.flush()
+            with open(self.f.name) as fh:
+                n = sum(1 for _ in fh)
+            if n:
+                self.skip = n
+                break
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
         if self.p:
+            # at least one sample from the timed region (or the instant after it)
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 0.5 and self.p.poll() is None:
+                self.f.flush()
+                with open(self.f.name) as fh:
+                    if sum(1 for _ in fh) > self.skip:
+                        break
+                time.sleep(0.01)
             self.p.terminate()
             try:
                 self.p.wait(timeout=5)
@@ -143,9 +163,9 @@ class Clocks:
         self.f.flush()
         rows = []
         try:
-            for line in open(self.f.name):
+            for i, line in enumerate(open(self.f.name)):
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
+                if i >= self.skip and len(parts) >= 9:
                     rows.append(parts)
         finally:
             os.unlink(self.f.name)
