@@ -1,7 +1,7 @@
 /*
  * analogsat_b200.h -- C ABI of the B200 (sm_100a) AnalogSAT CTDS solver.
  *
- * The reference library's boundary is a C++ template API (AnalogSAT/solver/*.h):
+ * The reference library's boundary is a C++ template API (the AnalogSAT/solver headers):
  * SatProblem + CnfReader/CnfWriter for the CNF, ISat (the ODE right-hand side and
  * clause check), IODEInt (the RK45 integrator) and SatSolver (the run-to-solution
  * loop).  This header exports that functionality as plain `extern "C"` calls:
