@@ -91,34 +91,65 @@ bool read_cnf(const char* path, HostProblem& p, std::string& msg) {
     if (!read_cnf_header(f, n, m, msg)) { std::fclose(f); return false; }
     p = HostProblem();
     if (n == 0 || m == 0) { msg = "empty problem"; std::fclose(f); return true; }
-    std::vector<int32_t> lits, lens;
-    lits.reserve(std::min<size_t>((size_t)m * 3, (size_t)1 << 24));  // the header may overstate M
-    lens.reserve(std::min<size_t>((size_t)m, (size_t)1 << 22));
-    int read = 0;
-    while (read < m) {
-        int len = 0;
-        while (true) {
-            long lit;
-            if (std::fscanf(f, "%ld", &lit) != 1) {
-                msg = "expected more literals in file";
-                std::fclose(f);
-                return false;
-            }
-            if (lit > 2147483647L || lit < -2147483647L) {
-                msg = "literal out of range";
-                std::fclose(f);
-                return false;
-            }
-            if (lit == 0) break;
-            lits.push_back((int32_t)lit);
-            len++;
-        }
-        lens.push_back(len);
-        read++;
-    }
+    // the rest of the file in one read, then the clause body by fscanf's rules
+    std::vector<char> body;
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) body.insert(body.end(), chunk, chunk + got);
     std::fclose(f);
-    p.add_clauses(lits.data(), lens.data(), (int)lens.size());
+    std::vector<int32_t> lits, lens;
+    if (!parse_cnf_body_host(body.data(), body.size(), m, lits, lens, msg)) return false;
+    p.set_clauses(std::move(lits), lens);
     msg = "read ok";
+    return true;
+}
+
+// CnfReader.cpp:100-127 reads the body with fscanf("%d") until M zeros are read:
+// skip white space (C locale), an optional sign, at least one digit, greedily.  The
+// same reads here over the bytes in memory, with "%ld"'s range checked instead of
+// "%d"'s undefined overflow.
+bool parse_cnf_body_host(const char* b, size_t len, long long m, std::vector<int32_t>& lits,
+                         std::vector<int32_t>& lens, std::string& msg) {
+    auto space = [](unsigned char c) { return c == ' ' || (c >= '\t' && c <= '\r'); };
+    auto digit = [](unsigned char c) { return c >= '0' && c <= '9'; };
+    lits.clear();
+    lens.clear();
+    lits.reserve(std::min<size_t>(len / 2 + 1, (size_t)m * 3));
+    lens.reserve(std::min<size_t>(len / 2 + 1, (size_t)m));
+    size_t i = 0;
+    int cur = 0;
+    long long zeros = 0;
+    while (zeros < m) {
+        while (i < len && space((unsigned char)b[i])) i++;
+        bool neg = false;
+        if (i < len && (b[i] == '+' || b[i] == '-')) {
+            neg = b[i] == '-';
+            i++;
+        }
+        if (i >= len || !digit((unsigned char)b[i])) {
+            msg = "expected more literals in file";
+            return false;
+        }
+        long long v = 0;
+        bool range = false;
+        for (; i < len && digit((unsigned char)b[i]); i++)
+            if (!range) {
+                v = v * 10 + (b[i] - '0');
+                range = v > 2147483647LL;
+            }
+        if (range) {
+            msg = "literal out of range";
+            return false;
+        }
+        if (v == 0) {
+            lens.push_back(cur);
+            cur = 0;
+            zeros++;
+        } else {
+            lits.push_back((int32_t)(neg ? -v : v));
+            cur++;
+        }
+    }
     return true;
 }
 

@@ -70,6 +70,12 @@ bool read_cnf(const char* path, HostProblem& p, std::string& msg);
 // "p cnf N M" declaration and leaves f just after M.  Returns false with msg set when
 // the declaration is malformed or missing.
 bool read_cnf_header(std::FILE* f, int& n, int& m, std::string& msg);
+// The clause body (the bytes after the header) read as CnfReader::Read reads it,
+// fscanf-style, from memory: the first m zero-terminated clauses (empty ones
+// included).  False with msg "expected more literals in file" or "literal out of
+// range" at the first read that fails.
+bool parse_cnf_body_host(const char* body, size_t len, long long m, std::vector<int32_t>& literals,
+                         std::vector<int32_t>& lengths, std::string& msg);
 // CnfWriter::Write (AnalogSAT/io/CnfWriter.cpp:49-74).
 bool write_cnf(const char* path, const HostProblem& p);
 

@@ -151,3 +151,35 @@ def test_rule_matches_host_reader_on_mutations(tmp_path):
         if i % 40 == 39:
             data = data[: int(rng.integers(body0, len(data)))]
         _check(tmp_path, bytes(data), f"m{i}.cnf")
+
+
+def test_rule_matches_host_reader_on_the_device_test_mutations(tmp_path):
+    """The 300 mutated files of test_gpu_ingest.py's device-reader test (same
+    generator and seed), so that the device reader, the host reader and the rule are
+    compared on one set."""
+    from analogsat_b200.instances import make_instance
+    lits, lens, _ = make_instance("random", 800, 3000, 3, seed=6)
+    base = formatted_cnf(lits, lens, seed=2)
+    start = base.index(b"\n", base.index(b"p cnf"))
+    body0 = start + 1
+    alphabet = b"0123456789-+ \n\t\r\x0bx%c\x00"
+    rng = np.random.default_rng(11)
+    for i in range(300):
+        data = bytearray(base)
+        for _ in range(int(rng.integers(1, 4))):
+            if i % 3 == 0:
+                pos = start + 4096 * int(rng.integers(1, (len(data) - start) // 4096 + 1)) + int(rng.integers(-2, 2))
+            else:
+                pos = int(rng.integers(body0, len(data)))
+            pos = min(max(pos, body0), len(data) - 1)
+            op = rng.integers(3)
+            ch = alphabet[int(rng.integers(len(alphabet)))]
+            if op == 0:
+                data[pos] = ch
+            elif op == 1:
+                data.insert(pos, ch)
+            else:
+                del data[pos:pos + int(rng.integers(1, 6))]
+        if i % 50 == 49:
+            data = data[: int(rng.integers(body0, len(data)))]
+        _check(tmp_path, bytes(data), f"d{i}.cnf")
