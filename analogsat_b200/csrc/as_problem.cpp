@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 
 namespace asb {
 
@@ -153,16 +154,32 @@ bool parse_cnf_body_host(const char* b, size_t len, long long m, std::vector<int
     return true;
 }
 
+// The text of CnfWriter::Write ("p cnf N M", then per clause "%d " per literal and
+// "0"), formatted into a buffer instead of one fprintf per literal.
 bool write_cnf(const char* path, const HostProblem& p) {
     FILE* f = std::fopen(path, "w");
     if (!f) return false;
-    std::fprintf(f, "p cnf %d %d\n", p.n, p.m);
+    std::string out;
+    out.reserve((size_t)p.storage.size() * 8 + (size_t)p.m * 2 + 64);
+    char buf[32];
+    out += "p cnf " + std::to_string(p.n) + " " + std::to_string(p.m) + "\n";
+    auto put_int = [&](int v) {
+        char* e = buf + sizeof buf;
+        char* q = e;
+        unsigned u = v < 0 ? 0u - (unsigned)v : (unsigned)v;
+        do { *--q = (char)('0' + u % 10); u /= 10; } while (u);
+        if (v < 0) *--q = '-';
+        out.append(q, e);
+    };
     for (int j = 0; j < p.m; j++) {
-        for (int i = 0; i < p.length[j]; i++) std::fprintf(f, "%d ", p.storage[p.start[j] + i]);
-        std::fprintf(f, "0\n");
+        for (int i = 0; i < p.length[j]; i++) {
+            put_int(p.storage[p.start[j] + i]);
+            out += ' ';
+        }
+        out += "0\n";
     }
-    std::fclose(f);
-    return true;
+    const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+    return std::fclose(f) == 0 && ok;
 }
 
 namespace {

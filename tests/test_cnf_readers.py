@@ -110,3 +110,26 @@ def test_philox_stream_matches_numpy():
         assert np.array_equal(g.random(256), u)
         g = np.random.Generator(np.random.Philox(key=seed))
         assert np.array_equal(g.uniform(-1.0, 1.0, 256), u * 2.0 - 1.0)
+
+
+def test_writer_matches_reference_writer_byte_for_byte(tmp_path):
+    """as_problem_write_cnf against the reference's CnfWriter: identical files, for a
+    3-SAT, a mixed-length and a k = 12 instance (negative literals, unused variables)."""
+    from analogsat_b200 import SatProblem
+    from analogsat_b200.instances import make_instance
+    R = _reference()
+    if R is None:
+        pytest.skip("reference checker not built here")
+    for kind, n, m, k, seed in [("random", 300, 1200, 3, 2), ("fast", 50, 40, 12, 1)]:
+        lits, lens, _ = make_instance(kind, n, m, k, seed=seed)
+        ours, ref = str(tmp_path / "ours.cnf"), str(tmp_path / "ref.cnf")
+        SatProblem.from_arrays(lits, lens).write_cnf(ours)
+        R.write_cnf(R.problem(lits, lens), ref)
+        assert open(ours, "rb").read() == open(ref, "rb").read()
+    clauses = [[1], [-2, 3], [4, -5, 6], [-1, 2, -3, 4, 5], [9, -9]]
+    lits = np.array([l for c in clauses for l in c], np.int32)
+    lens = np.array([len(c) for c in clauses], np.int32)
+    ours, ref = str(tmp_path / "ours.cnf"), str(tmp_path / "ref.cnf")
+    SatProblem.from_arrays(lits, lens).write_cnf(ours)
+    R.write_cnf(R.problem(lits, lens), ref)
+    assert open(ours, "rb").read() == open(ref, "rb").read()
