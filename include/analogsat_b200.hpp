@@ -201,6 +201,7 @@ public:
         for (auto* p : problems) {
             hs.push_back(p->handle());
             nm_.push_back(p->Get_N() + p->Get_M());
+            n_.push_back(p->Get_N());
         }
         as_solver* s = nullptr;
         check(as_solver_create(hs.data(), (int32_t)hs.size(), kPrecision, device, &s));
@@ -248,10 +249,41 @@ public:
         const auto t0 = std::chrono::steady_clock::now();
         check(as_solver_solve(s_.get()));
         wall_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        fetch();
-        std::vector<SatResult> r(status_.size());
-        for (size_t i = 0; i < r.size(); i++) r[i] = (SatResult)status_[i];
-        return r;
+        return results();
+    }
+    // Asynchronous form: enqueues the solve on `stream` (a cudaStream_t; null: the
+    // solver's own stream); Sync() waits for it and returns the SatResults.
+    void SolveAsync(void* stream = nullptr) { check(as_solver_solve_async(s_.get(), stream)); }
+    std::vector<SatResult> Sync() {
+        check(as_solver_sync(s_.get()));
+        return results();
+    }
+
+    // Launch shape (no reference counterpart): CTA size, storage mode (0 automatic,
+    // 1 shared memory, 2 global storage, 3 streamed).
+    void ForceThreads(int threads) { check(as_solver_force_threads(s_.get(), threads)); }
+    void SetStorageMode(int mode) { check(as_solver_set_storage_mode(s_.get(), mode)); }
+
+    // MAXSAT runs (SetTrackBest(true)): the Boolean assignment with the fewest unsat
+    // clauses seen by trajectory traj; element i is variable i + 1.
+    std::vector<bool> GetBestAssignment(int traj) const {
+        if (traj < 0 || traj >= (int)index_.size()) throw Error(AS_ERR_BAD_INPUT, "trajectory index out of range");
+        const int n = n_[index_[traj]];
+        std::vector<uint32_t> bits((n + 31) / 32);
+        check(as_solver_get_best_assignment(s_.get(), traj, bits.data()));
+        std::vector<bool> a(n);
+        for (int i = 0; i < n; i++) a[i] = (bits[i >> 5] >> (i & 31)) & 1u;
+        return a;
+    }
+
+    // The reference frontend's outputs: the MiniSat-compatible result file
+    // (cnf_runner.cpp:280-304) and the tab-separated perf line (bench_runner.cpp:331-343).
+    void WriteResult(int traj, const std::string& path) const {
+        check(as_solver_write_result(s_.get(), traj, path.c_str()));
+    }
+    void AppendPerf(int traj, const std::string& path, const std::string& sample,
+                    const std::string& solver_name) const {
+        check(as_solver_append_perf(s_.get(), traj, path.c_str(), sample.c_str(), solver_name.c_str()));
     }
 
     std::vector<TFloat> GetSatState(int traj) const {
@@ -275,7 +307,7 @@ public:
 
 private:
     std::shared_ptr<as_solver> s_;
-    std::vector<int> nm_;
+    std::vector<int> nm_, n_;
     std::vector<int32_t> index_;
     std::vector<int32_t> status_, steps_, rhs_, att_, viol_, minv_;
     std::vector<double> time_, hdid_;
@@ -285,6 +317,12 @@ private:
         size_t t = 0;
         for (auto i : index_) t += nm_[i];
         return t;
+    }
+    std::vector<SatResult> results() {
+        fetch();
+        std::vector<SatResult> r(status_.size());
+        for (size_t i = 0; i < r.size(); i++) r[i] = (SatResult)status_[i];
+        return r;
     }
     void fetch() {
         const size_t n = index_.size();
