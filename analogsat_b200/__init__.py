@@ -26,7 +26,7 @@ from ._abi import AnalogSatError, AS_PREC_F32_LOGA, AS_PREC_F64, check, load
 
 __all__ = [
     "SatResult", "SatProblem", "SatSolver", "AnalogSatError", "AS_PREC_F32_LOGA", "AS_PREC_F64",
-    "get_derivatives", "clause_violation_counts", "load", "sat_result_message",
+    "get_derivatives", "rhs_check", "clause_violation_counts", "load", "sat_result_message",
 ]
 
 
@@ -202,6 +202,12 @@ def get_derivatives(problem: SatProblem, x, out=None, logspace: bool = False, st
     else:
         raise AnalogSatError(_abi.AS_ERR_BAD_INPUT, "x must be float32 or float64")
     return out
+
+
+def rhs_check(problem: SatProblem, stream=None) -> None:
+    """Waits for `stream` and raises AnalogSatError(AS_ERR_TIMEOUT) if a device RHS on
+    `problem` gave up waiting for one of its bulk copies (its outputs then hold NaN)."""
+    check(load().as_rhs_check(problem._h, _stream_ptr(stream)))
 
 
 def clause_violation_counts(problem: SatProblem, x, stream=None):

@@ -18,6 +18,7 @@ AS_ERR_CUDA = -2
 AS_ERR_NO_PROBLEM = -3
 AS_ERR_UNSUPPORTED = -4
 AS_ERR_IO = -5
+AS_ERR_TIMEOUT = -6
 AS_PREC_F32_LOGA = 0
 AS_PREC_F64 = 1
 AS_LAYOUT_F32_PAIR = 2  # layout_stats only
@@ -51,6 +52,7 @@ SIGNATURES = [
     ("as_problem_free", None, [_vp]),
     ("as_rhs_f32", _i32, [_vp, _vp, _vp, _i32, _i32, _vp]),
     ("as_rhs_f64", _i32, [_vp, _vp, _vp, _i32, _vp]),
+    ("as_rhs_check", _i32, [_vp, _vp]),
     ("as_violations_f32", _i32, [_vp, _vp, _vp, _i32, _vp]),
     ("as_violations_f64", _i32, [_vp, _vp, _vp, _i32, _vp]),
     ("as_solver_create", _i32, [C.POINTER(_vp), _i32, _i32, _i32, C.POINTER(_vp)]),

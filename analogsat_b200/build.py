@@ -32,6 +32,23 @@ def headers() -> list[str]:
     return hs
 
 
+CLI_SRC = os.path.join(HERE, "frontend", "analogsat_cli.cpp")
+CLI = os.path.join(HERE, "analogsat-b200")
+
+
+def build_cli(force: bool = False) -> str:
+    """The command-line frontend (run / speedtest / bench) linked against the library."""
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    deps = [CLI_SRC, LIB, os.path.join(inc, "analogsat_b200.hpp"), os.path.join(inc, "analogsat_b200.h")]
+    if not force and os.path.exists(CLI) and all(os.path.getmtime(f) <= os.path.getmtime(CLI) for f in deps):
+        return CLI
+    cxx = os.environ.get("CXX", "g++")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-I", inc, CLI_SRC, "-o", CLI + ".tmp", "-L", HERE,
+                    "-lanalogsat_b200", "-Wl,-rpath,$ORIGIN"], check=True)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
@@ -40,8 +57,10 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the library if any source is newer than it; returns its path."""
+    """Compile the library (and the command-line frontend) if any source is newer than
+    it; returns the library's path."""
     if not force and up_to_date():
+        build_cli()
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
     cmd = [nvcc, *NVCC_FLAGS, "-o", LIB + ".tmp", *sources()]
@@ -50,6 +69,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
+    build_cli(force=True)
     return LIB
 
 

@@ -202,6 +202,16 @@ int preferred_bt(const PackedProblem& q) {
     return std::max(64, std::min(1024, bt));
 }
 
+// CTA size of a shared-memory launch: a trajectory of `vals` shared values that leaves
+// no room for a second CTA on its SM gets the largest CTA (more warps to hide the
+// clause phase's latencies), smaller ones `bt`.
+int shared_cta_threads(size_t vals, size_t bytes_per_value, int bt, int device, int* out) {
+    int per_sm = 0;
+    AS_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+    *out = 2 * (vals * bytes_per_value + 2048) > (size_t)per_sm ? 1024 : bt;
+    return AS_OK;
+}
+
 __global__ void stamp_deadline_kernel(unsigned long long* out, unsigned long long budget_ns) {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -223,6 +233,8 @@ struct as_problem {
     std::mutex mu_;
     DevicePool dev[3];        // lazily uploaded for the device primitives
     DevBuf slab[3];           // per-CTA storage of the global-storage primitives
+    DevBuf rhs_status;        // set by a device RHS whose bulk copy timed out (as_rhs_check)
+    int rhs_status_dev = -1;  // device holding rhs_status
 
     int tanh = 0;       // CTDS variant (ISat implementation) and its parameters
     double q = 1.1, b = 0.0;
@@ -297,6 +309,7 @@ struct as_solver {
 
     DevBuf states, results, unit_inst, unit_state, unit_bits, queue, solved, deadline, best_bits, slab;
     cudaStream_t stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;  // orders a caller's stream with `stream`
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
     bool groups_dirty = true;
@@ -304,6 +317,8 @@ struct as_solver {
 
     ~as_solver() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
         if (stream) cudaStreamDestroy(stream);
     }
     void invalidate() { graph_valid = false; }
@@ -545,8 +560,13 @@ int launch_rhs_pair(as_problem* p, const float* x, float* d, int ns, cudaStream_
     const int grid = std::max(1, std::min((ns + 1) / 2, sms * occ));
     // bulk stores need dxdt congruent with x mod 16 bytes (same staging offsets)
     const int bulk_out = ((reinterpret_cast<uintptr_t>(x) - reinterpret_cast<uintptr_t>(d)) & 15u) == 0;
+    if (p->rhs_status_dev != dev) {
+        AS_CUDA(p->rhs_status.alloc(sizeof(int)));
+        AS_CUDA(cudaMemset(p->rhs_status.p, 0, sizeof(int)));
+        p->rhs_status_dev = dev;
+    }
     fn<<<grid, BT, smem, st>>>(p->dev[kLayoutPair].host_inst[0], x, d, ns, (long long)(q.n + q.m),
-                               bulk_out);
+                               bulk_out, p->rhs_status.as<int>());
     AS_CUDA(cudaGetLastError());
     *done = true;
     return AS_OK;
@@ -615,6 +635,23 @@ int32_t as_rhs_f32(as_problem* p, const float* x, float* dxdt, int32_t num_state
                    void* stream) {
     return logspace ? dispatch_rhs<float, true>(p, x, dxdt, num_states, stream)
                     : dispatch_rhs<float, false>(p, x, dxdt, num_states, stream);
+}
+
+int32_t as_rhs_check(as_problem* p, void* stream) {
+    if (!p) return fail(AS_ERR_BAD_INPUT, "as_rhs_check: null problem");
+    AS_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (p->rhs_status_dev < 0) return AS_OK;  // no bulk-copy RHS has run
+    int dev = 0, word = 0;
+    AS_CUDA(cudaGetDevice(&dev));
+    if (dev != p->rhs_status_dev) AS_CUDA(cudaSetDevice(p->rhs_status_dev));
+    cudaError_t e = cudaMemcpy(&word, p->rhs_status.p, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && word) e = cudaMemset(p->rhs_status.p, 0, sizeof(int));
+    if (dev != p->rhs_status_dev) cudaSetDevice(dev);
+    if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("as_rhs_check: ") + cudaGetErrorString(e));
+    if (word)
+        return fail(AS_ERR_TIMEOUT, "as_rhs_f32: a bulk copy did not complete within 2 s; the states "
+                                    "of the affected CTA hold NaN");
+    return AS_OK;
 }
 
 int32_t as_rhs_f64(as_problem* p, const double* x, double* dxdt, int32_t num_states, void* stream) {
@@ -847,9 +884,8 @@ int build_groups(as_solver* s) {
         // the largest CTA (more warps to hide the clause phase's latencies)
         int sm_bt = bt;
         if (!v.gs) {
-            int per_sm = 0;
-            AS_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, s->device));
-            if (2 * (vals * v.bytes_per_value + 2048) > (size_t)per_sm) sm_bt = 1024;
+            const int r = shared_cta_threads(vals, v.bytes_per_value, bt, s->device, &sm_bt);
+            if (r) return r;
         }
         G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : gs_bt) : sm_bt);
         G.smem = v.gs ? 0 : vals * v.bytes_per_value;
@@ -1374,7 +1410,20 @@ int32_t as_solver_solve_async(as_solver* s, void* stream) {
         if (r) return r;
     }
     cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
-    if (st != s->stream) return record_solve(s, st);
+    if (st != s->stream) {
+        // The solve runs on the caller's stream: after the work already queued on the
+        // solver's stream (states copied in by as_solver_set_states_*), and before
+        // anything queued there later (as_solver_sync, result and state reads).
+        if (!s->ev_in) AS_CUDA(cudaEventCreateWithFlags(&s->ev_in, cudaEventDisableTiming));
+        if (!s->ev_out) AS_CUDA(cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming));
+        AS_CUDA(cudaEventRecord(s->ev_in, s->stream));
+        AS_CUDA(cudaStreamWaitEvent(st, s->ev_in, 0));
+        int r = record_solve(s, st);
+        if (r) return r;
+        AS_CUDA(cudaEventRecord(s->ev_out, st));
+        AS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_out, 0));
+        return AS_OK;
+    }
     if (!s->graph_valid) {
         if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
         cudaGraph_t g = nullptr;
@@ -1701,8 +1750,15 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
         const long score = variant_score(cand);
         if (best < 0 || score < best) { best = score; v = &cand; }
     }
-    if (!v) return fail(AS_ERR_UNSUPPORTED, "as_solver_solve_noalloc: no launch shape fits the problem");
-    const int bt = s->forced_bt ? s->forced_bt : preferred_bt(q);
+    if (!v)
+        return fail(AS_ERR_UNSUPPORTED, "as_solver_solve_noalloc: the instance does not fit one SM's shared "
+                                        "memory (only shared-memory launches need no device buffers)");
+    int bt = s->forced_bt;
+    if (!bt) {
+        r = shared_cta_threads(solve_smem_values(q.n, q.m, q.nslots), v->bytes_per_value,
+                               std::max(64, preferred_bt(q)), s->device, &bt);
+        if (r) return r;
+    }
     const size_t smem = solver_smem(*v, q);
     cudaStream_t st = (cudaStream_t)stream;
 

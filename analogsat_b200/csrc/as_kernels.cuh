@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
 // otherwise).  Two staging buffers alternate: pair i is stored from one while pair
 // i+1 lands in the other.  A wait that does not complete within two seconds (it
 // cannot, short of a broken device) turns every output of the CTA's remaining pairs
-// into NaN instead of hanging.
+// into NaN and sets *status to 1 instead of hanging.
 // Shared layout: 2 mbarriers | staging[2] (2 stride + 3 floats each) | sy2 | cs2.
 // ---------------------------------------------------------------------------
 __host__ __device__ inline size_t rhs2_stage_floats(long long stride) {
@@ -586,7 +586,8 @@ struct PairCopy {
 template <bool LOGA, int KMAX, bool EXACT, int BT, int CPT, int VPT>
 __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const float* __restrict__ x,
                                                           float* __restrict__ dxdt, int ntraj,
-                                                          long long stride, int bulk_out) {
+                                                          long long stride, int bulk_out,
+                                                          int* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw);
     const size_t sf = rhs2_stage_floats(stride);
@@ -655,7 +656,10 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
         const bool ok = mbar_wait_for(bar + b, (parity >> b) & 1u, kWaitNs);
         if (__syncthreads_or(!ok)) {
             mbar_wait_for(bar + b, (parity >> b) & 1u, kWaitNs);  // let a late copy land
-            if (tid == 0) bulk_wait_all();
+            if (tid == 0) {
+                bulk_wait_all();
+                atomicExch(status, 1);
+            }
             const float nan = __int_as_float(0x7fc00000);
             for (; pr < npairs; pr += G) {
                 const long long cnt = (2 * pr + 1 < ntraj ? 2 : 1) * stride;

@@ -24,7 +24,9 @@ final states inside the timed region).
 
 --impl reference times the reference AnalogSAT CPU solver (CpuSat<double> +
 CpuRungeKutta<double> driven by SatSolver, compiled from the reference's sources)
-with all host threads on a bounded sample of the same trajectories.
+with all host threads on a fixed sample of the same trajectories (trajectories 0
+and 1 of every instance, each run to its own SatResult; the GPU line's
+cpu_baseline is the same sample).
 
 Multi-GPU (torchrun, one process per GPU): replicas -- every rank solves its own
 64 instances x 256 trajectories (weak scaling, no data-path collective); the time
@@ -57,10 +59,15 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--instances", type=int, default=WORKLOAD["instances"])
     ap.add_argument("--traj", type=int, default=WORKLOAD["traj"])
-    ap.add_argument("--cpu-sample-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-rhs-bench", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the comparators (FP64, every trajectory, plain GPU path) and the "
+                         "other configurations (uneven batch, adjoint, MAXSAT)")
+    ap.add_argument("--plain-seconds", type=float, default=20.0,
+                    help="per precision: the plain GPU path starts runs while this budget lasts")
+    ap.add_argument("--extras-maxsat-seconds", type=float, default=10.0)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shape instead of the autotuned one")
     ap.add_argument("--threads", type=int, default=0,
@@ -179,36 +186,56 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(probs, pidx, ics, seconds: float, nthreads=None):
-    """Reference CPU solver (oracle/_ref) on the first trajectories of the workload,
-    all host threads, stop taking new trajectories after `seconds`."""
+# The reference CPU sample: trajectories 0 and 1 of every instance (128 runs for the
+# 64-instance workload), the same initial states the GPU solves, each run to its own
+# SatResult under the same step cap.  A fixed set of runs, none cut short, so the rate
+# does not depend on a time budget (a budget that drops long runs drops exactly the
+# heavy tail of slow starts and overstates the rate).
+CPU_SAMPLE_PER_INSTANCE = 2
+
+
+def cpu_sample_units(instances: int, traj: int, per_instance: int = CPU_SAMPLE_PER_INSTANCE):
+    """Unit indices of the CPU sample: trajectory j of instance i, j < per_instance, in
+    round-robin order over the instances."""
+    return np.array([i * traj + j for j in range(min(per_instance, traj)) for i in range(instances)],
+                    np.int64)
+
+
+def cpu_baseline(probs, pidx, ics, units, nthreads=None, maxsteps=None):
+    """Reference CPU solver (oracle/_ref: CpuSat<double> + CpuRungeKutta<double> driven by
+    SatSolver) on the given units of the workload, all host threads, every run to its own
+    SatResult.  The rate is solved runs per second of thread-busy time times the threads:
+    the runs' own wall seconds spread over the threads, so threads waiting idle for the
+    last run are not charged.  With one start per Solve() (the reference's plain
+    method), every solved run is one instance solved."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Reference
     R = Reference()
     W = WORKLOAD
-    T = len(pidx) // len(probs)
-    # spread the sample over instances: trajectory j of instance i in round-robin order
-    order = np.array([i * T + j for j in range(T) for i in range(len(probs))])
-    used = sorted(set(pidx[order[:4096]]))
-    rp = {i: R.problem(*probs[i]) for i in used}
-    handles = [rp[i] for i in used]
+    ics = ics.reshape(len(pidx), -1)
+    used = sorted(set(int(pidx[u]) for u in units))
     remap = {i: k for k, i in enumerate(used)}
-    nm = W["n"] + W["m"]
-    ics = ics.reshape(-1, nm)
-    sample = order[:4096]
-    units_p = np.array([remap[pidx[u]] for u in sample], np.int32)
-    units_x = [ics[u].astype(np.float64) for u in sample]
+    handles = [R.problem(*probs[i]) for i in used]
+    units_p = np.array([remap[int(pidx[u])] for u in units], np.int32)
+    units_x = [ics[u].astype(np.float64) for u in units]
     r = R.solve_many(handles, units_p, units_x, eps=W["eps"], tmax=W["tmax"],
-                     maxsteps=W["maxsteps"], batch=W["batch"], nthreads=nthreads,
-                     wall_budget=seconds)
-    done = r["done"].astype(bool)
-    solved = int(((r["result"] == 0) & done).sum())
-    rhs = int(r["rhs"][done].sum())
-    # rate with every thread busy: the completed runs' own wall seconds spread over the
-    # threads (idle threads waiting at the end of the sample are not charged)
-    busy = float(r["busy"][done].sum()) / r["threads"]
-    return dict(value=solved / busy, rhs_per_s=rhs / busy, wall=r["wall"],
-                completed=int(done.sum()), solved=solved, threads=r["threads"])
+                     maxsteps=maxsteps or W["maxsteps"], batch=W["batch"], nthreads=nthreads)
+    assert int(r["done"].sum()) == len(units), "every run of the sample completes"
+    solved = int((r["result"] == 0).sum())
+    busy = float(r["busy"].sum()) / r["threads"]
+    return dict(value=solved / busy, rhs_per_s=float(r["rhs"].sum()) / busy, wall=r["wall"],
+                busy=busy, runs=len(units), solved=solved, threads=r["threads"],
+                steps_mean=float(r["steps"].mean()), steps_median=float(np.median(r["steps"])),
+                rhs_per_solve=float(r["rhs"].sum()) / max(solved, 1))
+
+
+def cpu_sample_text(c, instances):
+    return (f"{c['runs']} runs = trajectories 0..{c['runs'] // instances - 1} of each of the "
+            f"{instances} instances (the GPU's own initial states), each run to its SatResult "
+            f"(max_steps {WORKLOAD['maxsteps']}), none cut short: {c['solved']} solved, mean "
+            f"{c['steps_mean']:.0f} / median {c['steps_median']:.0f} steps, {c['wall']:.1f} s wall; "
+            f"reference CpuSat<double>+CpuRungeKutta<double> via SatSolver, {c['threads']} threads on "
+            f"{cpu_name()}; rate = solved runs per second of thread-busy time x threads")
 
 
 def cpu_name():
@@ -226,34 +253,27 @@ def run_reference(args):
     if rank != 0:
         return
     probs, pidx, ics = make_workload(0, args.instances, args.traj)
-    vals, rhs = [], []
-    for i in range(args.warmup):
-        cpu_baseline(probs, pidx, ics, 2.0)
-    # a bounded sample per step (new trajectories stop at per_step seconds, running ones
-    # at twice that), so that the whole run stays within about two minutes
-    per_step = max(2.0, min(args.cpu_sample_seconds, 60.0 / max(args.steps, 1)))
-    for i in range(args.steps):
-        c = cpu_baseline(probs, pidx, ics, per_step)
-        vals.append(c)
-    v = float(np.mean([c["value"] for c in vals]))
-    wall = float(np.sum([c["wall"] for c in vals]))
+    units = cpu_sample_units(args.instances, args.traj)
+    threads = os.cpu_count() or 1
+    for i in range(args.warmup):  # untimed: the first runs of the sample, capped short
+        cpu_baseline(probs, pidx, ics, units[:threads], maxsteps=200)
+    # the timed steps: the fixed sample dealt over the K steps (run u in step u mod K),
+    # run back to back by all host threads; the value is over the whole sample
+    order = np.concatenate([units[k::args.steps] for k in range(args.steps)])
+    c = cpu_baseline(probs, pidx, ics, order)
     line = {
-        "impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s",
+        "impl": "reference", "metric": "solves/s", "value": c["value"], "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * wall / max(args.steps, 1), "higher_is_better": True,
+        "ms_per_step": 1000.0 * c["wall"] / max(args.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD["name"], "instances": args.instances,
-                   "trajectories_per_instance": args.traj, "eps": WORKLOAD["eps"],
-                   "batch": WORKLOAD["batch"], "max_steps": WORKLOAD["maxsteps"]},
-        "rhs_evals_per_s": float(np.mean([c["rhs_per_s"] for c in vals])),
-        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": vals[0]["threads"],
-                         "kind": "reference",
-                         "sample": f"first trajectories (round-robin over instances) of the "
-                                   f"workload, {per_step:.0f} s budget per step (runs past twice it "
-                                   f"stopped and left out; rate over thread-busy time), "
-                                   f"reference CpuSat<double>+CpuRungeKutta<double> via SatSolver, "
-                                   f"{vals[0]['threads']} threads on {cpu_name()}"},
-        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                   "trajectories_per_instance": args.traj, "N": WORKLOAD["n"], "M": WORKLOAD["m"],
+                   "K": WORKLOAD["k"], "eps": WORKLOAD["eps"], "batch": WORKLOAD["batch"],
+                   "max_steps": WORKLOAD["maxsteps"], "sample_runs": c["runs"]},
+        "rhs_evals_per_s": c["rhs_per_s"],
+        "cpu_baseline": {"value": c["value"], "unit": "solves/s", "cores": c["threads"],
+                         "kind": "reference", "sample": cpu_sample_text(c, args.instances)},
+        "e2e": {"value": c["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -396,6 +416,12 @@ def run_ours(args):
             dist.destroy_process_group()
         return
 
+    # comparators and the other configurations (one GPU only: they are reported
+    # beside the headline, not scaled)
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras = bench_extras(args, A, probs, probs_raw, pidx, ics, shape)
+
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -438,6 +464,14 @@ def run_ours(args):
                              "traffic is far below the algorithmic bytes"},
         "clocks": clocks,
     }
+    line.update(extras)
+    # the metric's own ratios: the batched solver against the plain GPU path
+    for name in ("f64", "f32"):
+        pg = line.get("plain_gpu_path", {}).get(name, {})
+        if pg.get("rhs_evals_per_s"):
+            pg["ratio_rhs_evals"] = line["rhs_evals_per_s"] / pg["rhs_evals_per_s"]
+            pg["ratio_solves"] = (line["value"] / pg["instances_solved_per_s"]
+                                  if pg.get("instances_solved_per_s") else None)
     if e2e:
         line["e2e"] = e2e
     if rhs_line:
@@ -446,21 +480,118 @@ def run_ours(args):
         line["rhs_roofline"] = rhs_line
     if world == 1 and not args.no_cpu_baseline:
         try:
-            c = cpu_baseline(probs_raw, pidx, ics, args.cpu_sample_seconds)
+            c = cpu_baseline(probs_raw, pidx, ics, cpu_sample_units(args.instances, args.traj))
             line["cpu_baseline"] = {
                 "value": c["value"], "unit": "solves/s", "cores": c["threads"], "kind": "reference",
-                "rhs_evals_per_s": c["rhs_per_s"],
-                "sample": f"{c['completed']} trajectories (round-robin over the 64 instances) in "
-                          f"{c['wall']:.1f} s, reference CpuSat<double>+CpuRungeKutta<double> via "
-                          f"SatSolver, {c['threads']} threads on {cpu_name()}; solves per second "
-                          f"of thread-busy time x threads (runs past twice the "
-                          f"{args.cpu_sample_seconds:.0f} s budget stopped and left out)"}
+                "rhs_evals_per_s": c["rhs_per_s"], "rhs_per_solve": c["rhs_per_solve"],
+                "sample": cpu_sample_text(c, args.instances)}
         except Exception as e:  # the checker library may be absent on a foreign box
             line["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": 0,
                                     "kind": "reference", "sample": f"unavailable: {e}"}
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def timed_solves(A, probs, pidx, X, precision, stop_on_first, steps, shape=None):
+    """Our solver on the given trajectories of the headline instances: `steps` timed
+    solves after one warm-up, each from the same initial states (copied in on the
+    device before the timing), CUDA events around SolveAsync on its stream."""
+    import torch
+    W = WORKLOAD
+    s = A.SatSolver(probs, precision=precision)
+    s.SetEpsilon(W["eps"]); s.SetBatchSize(W["batch"]); s.SetMaxSteps(W["maxsteps"]); s.SetMaxTime(W["tmax"])
+    s.SetStopOnFirst(stop_on_first)
+    if shape and precision == A.AS_PREC_F32_LOGA:
+        s.ForceThreads(shape["threads"])
+        s.SetStorageMode(shape["storage"])
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    st = torch.cuda.Stream()
+    ms, solved, inst, rhs, steps_solved = 0.0, 0, 0, 0, []
+    for k in range(steps + 1):
+        s.SetSatStates(pidx, Xd, stream=st.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.SolveAsync(stream=st.cuda_stream)
+        e1.record(st)
+        st.synchronize()
+        if k == 0:
+            continue  # warm-up: launch groups and graph
+        r = s.results()
+        ms += e0.elapsed_time(e1)
+        solved += int((r["status"] == 0).sum())
+        inst += len(set(pidx[r["status"] == 0]))
+        rhs += int(r["rhs"].sum())
+        steps_solved += list(r["steps"][r["status"] == 0])
+    sec = ms / 1e3
+    out = {"seconds": sec, "steps": steps, "trajectories": int(len(pidx)),
+           "instances_solved_per_s": inst / sec, "trajectory_solves_per_s": solved / sec,
+           "rhs_evals_per_s": rhs / sec,
+           "median_steps_of_solved_trajectories": float(np.median(steps_solved)) if steps_solved else None,
+           "launch_shape": s.launch_shape()}
+    del s, Xd
+    return out
+
+
+def plain_gpu_path(probs_raw, pidx, ics, units, precision, budget):
+    """The reference's own CUDA path, the "plain GPU path": CudaSat1<T> + CudaRungeKutta<T>
+    driven by SatSolver, one instance and one trajectory per Solve() in sequence, as the
+    reference frontend runs it (Frontend/src/cnf_runner.cpp:28-127), built for sm_100a
+    from the reference sources (oracle/_ref/libanalogsat_refcuda.so).  Runs the given
+    units in order, starting new ones while the budget lasts; every started run goes to
+    its own SatResult."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefCuda
+    W = WORKLOAD
+    X = ics.reshape(len(pidx), -1)
+    R = RefCuda()
+    r = R.solve_many(probs_raw, pidx[units], [X[u].astype(np.float64) for u in units], precision=precision,
+                     eps=W["eps"], tmax=W["tmax"], maxsteps=W["maxsteps"], batch=W["batch"], wall_budget=budget)
+    d = int(r["done"])
+    solved = int((r["result"][:d] == 0).sum())
+    return {"instances_solved_per_s": solved / r["wall"], "rhs_evals_per_s": float(r["rhs"][:d].sum()) / r["wall"],
+            "runs": d, "solved": solved, "seconds": r["wall"],
+            "mean_steps": float(r["steps"][:d].mean()) if d else None,
+            "sample": f"trajectory 0 of instances 0, 1, 2, ... of the headline workload (its initial states), "
+                      f"started while a {budget:.0f} s budget lasted, each run to its SatResult"}
+
+
+def bench_extras(args, A, probs, probs_raw, pidx, ics, shape):
+    """Comparators of the headline and the other configurations, as extra keys."""
+    out = {}
+    W = WORKLOAD
+    nm = W["n"] + W["m"]
+
+    def guarded(key, fn):
+        try:
+            out[key] = fn()
+        except Exception as e:  # one failed extra must not lose the headline line
+            out[key] = {"error": f"{type(e).__name__}: {e}"}
+
+    # FP64 on the headline workload (global-storage mode: an FP64 trajectory of this
+    # size does not fit one SM's shared memory)
+    guarded("f64", lambda: dict(timed_solves(A, probs, pidx, ics.astype(np.float64), A.AS_PREC_F64, True, 2),
+                                mode="first solution per instance stops its other trajectories"))
+    # every trajectory to its own SatResult (the like-for-like with the reference's
+    # one start per Solve()): trajectories 0..7 of every instance
+    units = cpu_sample_units(args.instances, args.traj, 8)
+    guarded("all_trajectories", lambda: dict(
+        timed_solves(A, probs, pidx[units], ics.reshape(-1, nm)[units], A.AS_PREC_F32_LOGA, False, 2, shape),
+        mode="trajectories 0..7 of every instance, each to its own SatResult"))
+    # the plain GPU path in both precisions, on the first trajectories of the workload
+    plain_units = cpu_sample_units(args.instances, args.traj, 2)
+    for name, prec in (("f64", 1), ("f32", 0)):
+        guarded(f"plain_{name}", lambda prec=prec: plain_gpu_path(probs_raw, pidx, ics, plain_units, prec,
+                                                                    args.plain_seconds))
+    plain = {"kernel_path": "reference CudaSat1<T> + CudaRungeKutta<T> via SatSolver, sm_100a"}
+    for name in ("f64", "f32"):
+        plain[name] = out.pop(f"plain_{name}")
+    out["plain_gpu_path"] = plain
+    # the other configurations
+    guarded("uneven", lambda: bench_uneven(2, WORKLOAD["maxsteps"]))
+    guarded("adjoint", bench_adjoint)
+    guarded("maxsat", lambda: bench_maxsat(args.extras_maxsat_seconds))
+    return out
 
 
 def rhs_kernel_bench(A, problem, ics_dev, nm, st, reps=10):
@@ -512,6 +643,10 @@ def verify_solutions(solver, probs_raw, pidx, r, nm):
 
 
 def run_uneven(args):
+    print(json.dumps(bench_uneven(args.steps, args.max_steps)), flush=True)
+
+
+def bench_uneven(steps: int, max_steps: int):
     """512 planted 3-SAT instances of uneven size, 64 trajectories each, first solution per
     instance stops the rest; the whole batch is one graph-captured solve call (shared-
     memory launch group for instances that fit one SM, global-storage group for the rest)."""
@@ -530,7 +665,7 @@ def run_uneven(args):
         raw.append((lits, lens)); sizes.append((n, m))
     probs = [A.SatProblem.from_arrays(l, c) for l, c in raw]
     s = A.SatSolver(probs)
-    s.SetEpsilon(1e-6); s.SetBatchSize(50); s.SetMaxSteps(args.max_steps); s.SetMaxTime(1e8)
+    s.SetEpsilon(1e-6); s.SetBatchSize(50); s.SetMaxSteps(max_steps); s.SetMaxTime(1e8)
     s.SetStopOnFirst(True)
     pidx = np.repeat(np.arange(P), T).astype(np.int32)
     X = np.concatenate([initial_states(n, m, T, seed=40_000 + i, dtype=np.float32)
@@ -540,7 +675,7 @@ def run_uneven(args):
     s.Solve()  # warm-up: builds launch groups, captures the graph
     shape = s.launch_shape()
     walls, solved, rhs = [], 0, 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         s.SetSatStates(pidx, X)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
@@ -551,15 +686,19 @@ def run_uneven(args):
         rhs += int(r["rhs"].sum())
     wall = sum(walls)
     small = sum(1 for p in probs if p.layout_stats()["compact"] and p.n <= 1200)
-    print(json.dumps({"workload": "uneven-planted-3sat-512-inst-N100-5000-x64-traj", "instances": P,
-                      "trajectories_per_instance": T, "solves/s": solved / wall,
-                      "instances_solved_fraction": solved / (P * args.steps),
-                      "rhs_evals_per_s": rhs / wall, "ms_per_solve_call": 1000 * wall / args.steps,
-                      "setup_s": setup, "last_group_launch_shape": shape,
-                      "instances_N_le_1200": small}), flush=True)
+    return {"workload": "uneven-planted-3sat-512-inst-N100-5000-x64-traj", "instances": P,
+            "trajectories_per_instance": T, "solves/s": solved / wall,
+            "instances_solved_fraction": solved / (P * steps),
+            "rhs_evals_per_s": rhs / wall, "ms_per_solve_call": 1000 * wall / steps, "steps": steps,
+            "setup_s": setup, "last_group_launch_shape": shape, "instances_N_le_1200": small,
+            "timing": "wall clock around each Solve() (states set before, outside the timing)"}
 
 
 def run_maxsat(args):
+    print(json.dumps(bench_maxsat(args.maxsat_seconds, args.maxsat_steps)), flush=True)
+
+
+def bench_maxsat(seconds: float, max_steps: int = 0):
     """One random 4-SAT instance N=1e5, M=1e6 (alpha 10, unsatisfiable w.h.p.), 32
     trajectories, minimise the unsat-clause count within a wall-clock budget; the best
     assignment of every trajectory is kept on device and re-counted exactly here."""
@@ -569,10 +708,10 @@ def run_maxsat(args):
     lits, lens, _ = make_instance("fast", n, m, k, seed=5000)
     p = A.SatProblem.from_arrays(lits, lens)
     s = A.SatSolver([p])
-    steps = args.maxsat_steps if args.maxsat_steps > 0 else 10 ** 9
+    steps = max_steps if max_steps > 0 else 10 ** 9
     s.SetEpsilon(1e-6); s.SetBatchSize(min(10, steps)); s.SetMaxSteps(steps); s.SetMaxTime(1e30)
     s.SetTrackBest(True)
-    s.SetWallBudget(args.maxsat_seconds)
+    s.SetWallBudget(seconds)
     X = initial_states(n, m, T, seed=50_000, dtype=np.float32)
     s.SetSatStates(np.zeros(T, np.int32), X)
     t0 = time.perf_counter()
@@ -594,8 +733,8 @@ def run_maxsat(args):
     # streamed mode, eight trajectories per lane group: the literal words are read once
     # per group and RHS, so B_rhs = 8(N+M) + 4KM/8 per trajectory and RHS
     b_rhs = 8 * (n + m) + 4 * k * m / 8
-    print(json.dumps({"workload": "maxsat-random-4sat-N1e5-M1e6-x32-traj", "wall_s": wall,
-                      "budget_s": args.maxsat_seconds, "min_unsat": int(min(exact)),
+    return {"workload": "maxsat-random-4sat-N1e5-M1e6-x32-traj", "wall_s": wall,
+                      "budget_s": seconds, "min_unsat": int(min(exact)),
                       "median_min_unsat": float(np.median(exact)), "steps_median": float(np.median(r["steps"])),
                       "rhs_evals_per_s": rhs_s,
                       "roofline": {"bound": "hbm", "achieved": rhs_s * b_rhs / 1e9, "peak": hbm_peak,
@@ -604,10 +743,14 @@ def run_maxsat(args):
                                            "clause weights and the contribution intermediate are extra HBM "
                                            "traffic B_rhs leaves out (~12 GB per pass of 192 RHS, "
                                            "profiles/stream_kernels_maxsat_N1e5_M1e6.md)"},
-                      "launch_shape": s.launch_shape()}), flush=True)
+                      "launch_shape": s.launch_shape()}
 
 
 def run_adjoint(args):
+    print(json.dumps(bench_adjoint()), flush=True)
+
+
+def bench_adjoint():
     """Gradients of V = sum w a K^2 at T=5 w.r.t. s(0), a(0) and per-clause weights for
     1024 random 3-SAT instances (N=200, M=850), FP32 and FP64; reports gradients per
     second, the FP32-vs-FP64 relative error, and one descent step on a(0) lowering V."""
@@ -638,14 +781,15 @@ def run_adjoint(args):
     X2[:, n:] = np.maximum(Xr[:, n:] - step * ga, 1e-3)
     s64.SetSatStates(np.arange(P, dtype=np.int32), X2)
     g2 = s64.Adjoint(5.0, weights=w)
-    print(json.dumps({"workload": "adjoint-random-3sat-N200-M850-x1024-T5",
+    return {"workload": "adjoint-random-3sat-N200-M850-x1024-T5",
                       "fp32_s": t32, "fp64_s": t64, "gradients_per_s_fp32": P / t32,
                       "gradients_per_s_fp64": P / t64, "median_steps": float(np.median(g64["nsteps"])),
                       "fp32_vs_fp64_rel_err_grad_x0": rel(g32["grad_x0"], g64["grad_x0"]),
                       "fp32_vs_fp64_rel_err_grad_w": rel(g32["grad_w"], g64["grad_w"]),
                       "fp32_vs_fp64_rel_err_loss": rel(g32["loss"], g64["loss"]),
                       "mean_loss_before_a0_step": float(g64["loss"].mean()),
-                      "mean_loss_after_a0_step": float(g2["loss"].mean())}), flush=True)
+                      "mean_loss_after_a0_step": float(g2["loss"].mean()),
+                      "timing": "wall clock around one as_solver_adjoint call after a warm-up call"}
 
 
 def run_ingest(args):

@@ -50,6 +50,8 @@ extern "C" {
 #define AS_ERR_NO_PROBLEM (-3)
 #define AS_ERR_UNSUPPORTED (-4)
 #define AS_ERR_IO (-5)
+/* a device-side wait gave up (as_rhs_check): the affected outputs hold NaN */
+#define AS_ERR_TIMEOUT (-6)
 
 /* numeric modes */
 #define AS_PREC_F32_LOGA 0 /* FP32 state, a_m held as log2 a_m, FP64 error norm + time */
@@ -131,6 +133,14 @@ int32_t as_rhs_f32(as_problem* p, const float* x, float* dxdt, int32_t num_state
                    int32_t logspace, void* stream);
 /* FP64 variant, linear a: bit-identical to CpuSat<double>::GetDerivatives. */
 int32_t as_rhs_f64(as_problem* p, const double* x, double* dxdt, int32_t num_states, void* stream);
+/* Device-side status of the earlier asynchronous as_rhs_* calls on p (no reference
+ * counterpart; the reference RHS has no waits).  The FP32 RHS moves states through
+ * shared memory with asynchronous bulk copies and waits for them at most two
+ * seconds; a copy that has not completed by then (a broken device, never a normal
+ * run) leaves NaN in the outputs of the states that CTA had left and sets a status
+ * word of the problem.  as_rhs_check waits for `stream`, reads and clears that word,
+ * and returns AS_ERR_TIMEOUT if it was set, else AS_OK. */
+int32_t as_rhs_check(as_problem* p, void* stream);
 
 /* ISat::GetClauseViolationCount over many states (CpuSat.cpp:136-173,
  * CudaSat1.cu:484-498).  x: DEVICE pointer to num_states public vectors (only the
@@ -252,7 +262,7 @@ int32_t as_solver_force_threads(as_solver* s, int32_t threads);
  * AS_STORAGE_AUTO picks the streamed solver when every instance has N + M >= 2^19
  * state elements, else shared memory when the instance fits one SM, else global
  * storage (a per-CTA slab in device memory); the others force one.
- * AS_STORAGE_STREAM: trajectories of an instance are grouped by four with their
+ * AS_STORAGE_STREAM: trajectories of an instance are grouped by eight with their
  * states interleaved in device memory, and every RK attempt runs as per-stage
  * kernels over the whole GPU, replayed from a CUDA graph; each trajectory keeps its
  * own step size and the reference's counters.  It is host driven: a solve returns
@@ -312,6 +322,11 @@ int32_t as_solver_adjoint(as_solver* s, double t_end, int32_t max_steps, const d
  *  - states: DEVICE array of num_traj public states (N+M values each, float for
  *    AS_PREC_F32_LOGA solvers, double for AS_PREC_F64), initial states in, final
  *    states out.  results: DEVICE array of num_traj as_unit_result.
+ *  - Only instances whose whole trajectory fits one SM's shared memory are accepted
+ *    (N=1000/M=4250 in FP32 does): the global-storage and streamed modes need
+ *    device buffers, so as_solver_set_storage_mode is not consulted and a larger
+ *    instance fails with AS_ERR_UNSUPPORTED.  The CTA size is the one
+ *    as_solver_solve picks for the same instance (or as_solver_force_threads').
  *  - The solver's settings apply (epsilon, max time/steps, batch size, wall budget,
  *    stop-on-first); best-assignment tracking is not available here.
  *  - Asynchronous on `stream`; results are valid once the stream reaches this point. */

@@ -29,8 +29,12 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 
 
-def build(reference_root: str | None = "/root/reference") -> None:
-    """Compile the C restatement, and the reference solver when its sources exist."""
+REFERENCE_ROOT = os.environ.get("ANALOGSAT_REF", "/root/reference")
+
+
+def build(reference_root: str | None = REFERENCE_ROOT) -> None:
+    """Compile the C restatement, and the reference solver when its sources exist
+    (the reference source tree comes from $ANALOGSAT_REF, default /root/reference)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if reference_root and os.path.isdir(reference_root):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "refcuda", f"REF={reference_root}"], check=True)

@@ -73,3 +73,45 @@ def test_adjoint_central_differences(oracle):
         dw = rng.normal(size=w.shape); dw /= np.linalg.norm(dw)
         fd = (oracle.fixed_loss(p, X[0], hs, w + eh * dw) - oracle.fixed_loss(p, X[0], hs, w - eh * dw)) / (2 * eh)
         assert abs(fd - g["grad_w"] @ dw) <= 1e-5 * max(abs(fd), 1e-3)
+
+
+def test_adjoint_config4_shape_64_directions(oracle):
+    """The differentiation configuration at its full shape: 1024 random 3-SAT
+    instances N=200, M=850, gradients at T=5 of all of them in one call (FP64 and
+    FP32).  Central differences (h = 1e-4) of the frozen-step map along 64 random unit
+    directions of x(0) and 64 of w, on four instances spread over the batch (FP64,
+    relative 1e-5); FP32 against FP64 over all 1024 (2-norm over every gradient
+    entry <= 1e-5, per instance <= 5e-4 for 99% of them)."""
+    from analogsat_b200 import SatProblem, SatSolver
+    from analogsat_b200.instances import make_instance, initial_states
+    P, n, m = 1024, 200, 850
+    raw = [make_instance("random", n, m, 3, seed=6000 + i)[:2] for i in range(P)]
+    X = np.concatenate([initial_states(n, m, 1, seed=60_000 + i) for i in range(P)])
+    w = np.random.default_rng(6).uniform(0.5, 1.5, size=P * m)
+    probs = [SatProblem.from_arrays(l, c) for l, c in raw]
+    g = {}
+    for prec, dt in ((1, np.float64), (0, np.float32)):
+        s = SatSolver(probs, precision=prec)
+        s.SetEpsilon(1e-6)
+        s.SetSatStates(np.arange(P, dtype=np.int32), X.astype(dt))
+        g[prec] = s.Adjoint(5.0, weights=w)
+    nm = n + m
+    rng = np.random.default_rng(64)
+    eh = 1e-4
+    for t in (0, 341, 682, 1023):
+        p = oracle.problem(*raw[t])
+        hs = g[1]["step_sizes"][t]
+        x0, wt = X[t], w[t * m:(t + 1) * m]
+        gx, gw = g[1]["grad_x0"][t * nm:(t + 1) * nm], g[1]["grad_w"][t * m:(t + 1) * m]
+        for _ in range(64):
+            d = rng.normal(size=nm); d /= np.linalg.norm(d)
+            fd = (oracle.fixed_loss(p, x0 + eh * d, hs, wt) - oracle.fixed_loss(p, x0 - eh * d, hs, wt)) / (2 * eh)
+            assert abs(fd - gx @ d) <= 1e-5 * max(abs(fd), 1e-3), (t, fd, gx @ d)
+            dw = rng.normal(size=m); dw /= np.linalg.norm(dw)
+            fd = (oracle.fixed_loss(p, x0, hs, wt + eh * dw) - oracle.fixed_loss(p, x0, hs, wt - eh * dw)) / (2 * eh)
+            assert abs(fd - gw @ dw) <= 1e-5 * max(abs(fd), 1e-3), (t, fd, gw @ dw)
+    for key, size in (("grad_x0", nm), ("grad_w", m)):
+        a, b = g[0][key], g[1][key]
+        assert _rel(a, b) <= 1e-5, (key, _rel(a, b))
+        per = np.array([_rel(a[t * size:(t + 1) * size], b[t * size:(t + 1) * size]) for t in range(P)])
+        assert np.quantile(per, 0.99) <= 5e-4, (key, np.quantile(per, 0.99))

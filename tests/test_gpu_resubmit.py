@@ -52,3 +52,29 @@ def test_same_map_new_values_and_new_map(precision):
     full = s.GetSatStates(dt).reshape(3, 780)
     for t in range(3):
         assert np.array_equal(s.GetSatState(t, dt), full[t])
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_solve_async_on_a_caller_stream_then_sync(precision):
+    """SolveAsync on a stream of the caller's after a host SetSatStates (queued on the
+    solver's own stream), then Sync() and the result reads: the solve starts after the
+    states are in place and Sync() returns after it, so the results equal a plain
+    Solve() of the same states."""
+    from analogsat_b200.instances import initial_states
+    probs = _setup(precision)
+    dt = np.float32 if precision == 0 else np.float64
+    pidx = np.repeat(np.arange(3), 40).astype(np.int32)
+    X = initial_states(150, 630, len(pidx), seed=7, dtype=dt)
+    ref = _solver(probs, precision)
+    ref.SetMaxSteps(3000)
+    ref.SetSatStates(pidx, X); ref.Solve()
+    side = torch.cuda.Stream()
+    for rep in range(2):  # the second round replays with the unit tables kept
+        s = _solver(probs, precision) if rep == 0 else s
+        s.SetMaxSteps(3000)
+        s.SetSatStates(pidx, X)
+        s.SolveAsync(stream=side.cuda_stream)
+        s.Sync()
+        for key in ("status", "steps", "rhs", "violations"):
+            assert np.array_equal(s.results()[key], ref.results()[key]), (rep, key)
+        assert np.array_equal(s.GetSatStates(dt), ref.GetSatStates(dt))

@@ -171,3 +171,55 @@ def test_model_variants_bit_exact(oracle, golden, golden_models, tag, name):
         assert np.array_equal(tr["time"], golden_models[f"{tag}/{name}/traj_time"])
         assert np.array_equal(tr["rhs"], golden_models[f"{tag}/{name}/traj_rhs"])
         assert np.array_equal(tr["states"][-1], golden_models[f"{tag}/{name}/traj_final"])
+
+
+# Failure-path initial states, injected on the host: a NaN or infinite spin or clause
+# weight, every weight infinite or zero, and negative weights, whose dynamics blow up
+# in finite time so that the step size underflows (SAT_UNDERFLOW, CpuRungeKutta.cpp:
+# 246-248, SatSolver.h:322).  Also the smallest epsilon SetEpsilon accepts (1e-16).
+FAILURE_CASES = {
+    "nan_spin": (3, np.nan), "inf_spin": (3, np.inf), "neg_inf_weight": (60, -np.inf),
+    "nan_weight": (60, np.nan), "inf_weights": (slice(50, None), np.inf),
+    "zero_weights": (slice(50, None), 0.0), "negative_weights": (slice(50, None), -1.0),
+}
+
+
+def failure_ic(golden, case):
+    x = golden["p50/solve_ics"][0].copy()
+    where, val = FAILURE_CASES[case]
+    x[where] = val
+    return x
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference checker not built here")
+@pytest.mark.parametrize("case", sorted(FAILURE_CASES) + ["eps_1e-16"])
+def test_oracle_failure_paths_vs_live_reference(oracle, golden, case):
+    """The oracle reproduces the reference solver's SatResult, counters, time and final
+    state on the failure-path inputs (the reference's NaN handling included: fmax
+    skips NaN error ratios, CpuRungeKutta.cpp:236)."""
+    from oracle import Reference
+    R = Reference()
+    lits, lens = golden["p50/literals"], golden["p50/lengths"]
+    rp, op = R.problem(lits, lens), oracle.problem(lits, lens)
+    eps = 1e-16 if case == "eps_1e-16" else 1e-6
+    x = golden["p50/solve_ics"][0] if case == "eps_1e-16" else failure_ic(golden, case)
+    a = R.solve(rp, x, eps=eps, maxsteps=20000, batch=50, tmax=1e8)
+    b = oracle.solve(op, x, eps=eps, maxsteps=20000, batch=50, tmax=1e8)
+    for k in ("result", "steps", "rhs", "violations", "time"):
+        assert a[k] == b[k], (case, k, a[k], b[k])
+    assert np.array_equal(a["state"], b["state"], equal_nan=True)
+    if case == "negative_weights":
+        assert a["result"] == 1  # SAT_UNDERFLOW
+
+
+def test_minisat_fixture_certificates():
+    """The MiniSat verdict fixture (tests/golden/make_golden_stats.py): every SAT verdict
+    carries a model that satisfies its instance exactly; both verdicts occur."""
+    from analogsat_b200.instances import is_satisfied
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "minisat_3sat.npz")))
+    n, m, k = (int(v) for v in d["nmk"])
+    assert set(np.unique(d["verdict"])) == {10, 20}
+    for i, v in enumerate(d["verdict"]):
+        if v == 10:
+            assert is_satisfied(d["literals"][i].astype(np.int32), np.full(m, k, np.int32),
+                                d["model"][i].astype(bool))

@@ -33,11 +33,16 @@ def _solver(problem, precision, stop_on_first):
     return s
 
 
-@pytest.mark.parametrize("precision,stop_on_first", [(0, False), (0, True), (1, False)])
-def test_noalloc_matches_allocating_solve(precision, stop_on_first):
+# (precision, stop_on_first, N, M, trajectories): N=1000/M=4250 leaves no room for a
+# second CTA on an SM, so both entry points must pick the 1,024-thread CTA for it
+CASES = [(0, False, 200, 850, 96), (0, True, 200, 850, 96), (1, False, 200, 850, 96),
+         (0, False, 1000, 4250, 24)]
+
+
+@pytest.mark.parametrize("precision,stop_on_first,n,m,T", CASES)
+def test_noalloc_matches_allocating_solve(precision, stop_on_first, n, m, T):
     from analogsat_b200 import SatProblem, _abi
     from analogsat_b200.instances import make_instance, initial_states
-    n, m, T = 200, 850, 96
     lits, lens, _ = make_instance("planted", n, m, 3, seed=77)
     p = SatProblem.from_arrays(lits, lens)
     dt = np.float32 if precision == 0 else np.float64
@@ -55,10 +60,16 @@ def test_noalloc_matches_allocating_solve(precision, stop_on_first):
     for call in range(2):
         x = torch.from_numpy(ics.copy()).cuda()
         res = torch.zeros(T * RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         rc = lib.as_solver_solve_noalloc(s._h, 0, T, C.c_void_p(x.data_ptr()),
                                          C.c_void_p(res.data_ptr()), C.c_void_p(stream.cuda_stream))
         assert rc == 0, _abi.last_error()
         torch.cuda.synchronize()
+        if call == 1:
+            # the first call has loaded everything it needs: the second takes no device
+            # memory at all
+            assert torch.cuda.mem_get_info()[0] == free0
         r = np.frombuffer(res.cpu().numpy().tobytes(), dtype=RESULT_DTYPE)
         if stop_on_first:
             # which trajectory wins the race depends on CTA scheduling: compare the
@@ -78,6 +89,29 @@ def test_noalloc_matches_allocating_solve(precision, stop_on_first):
         np.testing.assert_allclose(x.cpu().numpy(), x_ref, rtol=1e-6, atol=1e-7)
 
 
+def test_noalloc_with_a_wall_budget_ends_with_valid_statuses():
+    """The wall-clock deadline lives in the static scratch too: a budget far shorter
+    than the run stops every trajectory with a valid SatResult."""
+    from analogsat_b200 import SatProblem, _abi
+    from analogsat_b200.instances import make_instance, initial_states
+    n, m, T = 1000, 4250, 300
+    lits, lens, _ = make_instance("random", n, m, 3, seed=9)
+    s = _solver(SatProblem.from_arrays(lits, lens), 0, False)
+    s.SetMaxSteps(1_000_000)
+    s.SetWallBudget(0.05)
+    lib = _abi.load()
+    for call in range(2):
+        x = torch.from_numpy(initial_states(n, m, T, seed=call, dtype=np.float32)).cuda()
+        res = torch.zeros(T * RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+        rc = lib.as_solver_solve_noalloc(s._h, 0, T, C.c_void_p(x.data_ptr()),
+                                         C.c_void_p(res.data_ptr()), None)
+        assert rc == 0, _abi.last_error()
+        torch.cuda.synchronize()
+        r = np.frombuffer(res.cpu().numpy().tobytes(), dtype=RESULT_DTYPE)
+        assert set(np.unique(r["status"])) <= {0, 2}, np.unique(r["status"])
+        assert (r["status"] == 2).any()  # 1e6 steps cannot finish in 50 ms
+
+
 def test_noalloc_rejects_oversize_requests():
     from analogsat_b200 import SatProblem, _abi
     from analogsat_b200.instances import make_instance
@@ -91,3 +125,10 @@ def test_noalloc_rejects_oversize_requests():
     rc = lib.as_solver_solve_noalloc(s._h, 1, 4, C.c_void_p(dummy.data_ptr()),
                                      C.c_void_p(dummy.data_ptr()), None)
     assert rc == _abi.AS_ERR_BAD_INPUT
+    # an instance beyond one SM's shared memory needs the device buffers of the
+    # global-storage mode, which this entry point does not have
+    big, bl, _ = make_instance("random", 6000, 25000, 3, seed=2)
+    s2 = _solver(SatProblem.from_arrays(big, bl), 0, False)
+    rc = lib.as_solver_solve_noalloc(s2._h, 0, 4, C.c_void_p(dummy.data_ptr()),
+                                     C.c_void_p(dummy.data_ptr()), None)
+    assert rc == _abi.AS_ERR_UNSUPPORTED and "shared memory" in _abi.last_error()
