@@ -270,6 +270,11 @@ class SatSolver:
     def ForceThreads(self, threads: int):
         check(self._lib.as_solver_force_threads(self._h, int(threads)))
 
+    def SetKernel(self, kernel: int):
+        """Shared-memory solver kernel: _abi.AS_KERNEL_AUTO (the lean FP32 kernel where the
+        instance qualifies) or _abi.AS_KERNEL_GENERIC."""
+        check(self._lib.as_solver_set_kernel(self._h, int(kernel)))
+
     def SetClusterSize(self, ctas: int):
         """CTAs per trajectory in global-storage mode: 0 automatic, 1, 4 or 8."""
         check(self._lib.as_solver_set_cluster_size(self._h, int(ctas)))

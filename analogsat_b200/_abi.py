@@ -22,6 +22,8 @@ AS_ERR_TIMEOUT = -6
 AS_PREC_F32_LOGA = 0
 AS_PREC_F64 = 1
 AS_LAYOUT_F32_PAIR = 2  # layout_stats only
+AS_KERNEL_AUTO = 0
+AS_KERNEL_GENERIC = 1
 AS_MODEL_CTDS = 0
 AS_MODEL_TANH = 1
 
@@ -80,6 +82,7 @@ SIGNATURES = [
     ("as_solver_get_best_assignment", _i32, [_vp, _i32, _vp]),
     ("as_solver_get_launch_shape", _i32, [_vp, _pi32, _pi32, _pi32, _pi32]),
     ("as_solver_force_threads", _i32, [_vp, _i32]),
+    ("as_solver_set_kernel", _i32, [_vp, _i32]),
     ("as_solver_set_storage_mode", _i32, [_vp, _i32]),
     ("as_solver_set_cluster_size", _i32, [_vp, _i32]),
     ("as_solver_set_stream_parts", _i32, [_vp, _i32]),

@@ -18,6 +18,7 @@
 
 #include "../../include/analogsat_b200.h"
 #include "as_ingest.h"
+#include "as_fast.cuh"
 #include "as_kernels.cuh"
 #include "as_problem.h"
 #include "as_stream.cuh"
@@ -65,7 +66,7 @@ struct DevBuf {
 // Device copy of one or more packed instances in a single pool.
 struct DevicePool {
     int device = -1;
-    DevBuf lit, litw, slotw, srow, perm, iperm, icperm, cperm, inst;
+    DevBuf lit, litw, slotw, srow, perm, iperm, icperm, cperm, inst, flit;
     std::vector<DevInstance> host_inst;
 
     template <typename V>
@@ -94,6 +95,26 @@ struct DevicePool {
         AS_CUDA(icperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(cperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
+        // clause-major literal words with shared-memory byte offsets for the lean FP32
+        // solver, for the instances whose offsets fit (bits 0-13 spin, 14-29 slot, 31 sign)
+        std::vector<uint32_t> fw;
+        std::vector<long long> fw_off;
+        for (auto* q : pk) {
+            const FastLayout L = fast_layout(q->n, q->m, q->nslots);
+            if (!q->compact || (q->k != 3 && q->k != 4) || !L.ok) {
+                fw_off.push_back(-1);
+                continue;
+            }
+            fw_off.push_back((long long)fw.size());
+            for (int c = 0; c < q->m; c++)
+                for (int qq = 0; qq < q->k; qq++) {
+                    const uint32_t w = q->lit[(size_t)qq * q->mp + c];
+                    const uint32_t var = (w >> 16) & 0x7fffu, slot = w & 0xffffu;
+                    fw.push_back((w & 0x80000000u) | (((uint32_t)L.cs_off + 4u * slot) << 14) | (4u * var));
+                }
+        }
+        AS_CUDA(flit.alloc(std::max<size_t>(fw.size(), 1) * 4));
+        if (!fw.empty()) AS_CUDA(cudaMemcpy(flit.p, fw.data(), fw.size() * 4, cudaMemcpyHostToDevice));
         host_inst.clear();
         size_t ol = 0, ow = 0, orr = 0, op = 0, oc = 0;
         for (auto* q : pk) {
@@ -111,6 +132,13 @@ struct DevicePool {
             d.iperm = iperm.as<int32_t>() + op;
             d.icperm = icperm.as<int32_t>() + oc;
             d.cperm = cperm.as<int32_t>() + oc;
+            {
+                const FastLayout L = fast_layout(q->n, q->m, q->nslots);
+                const long long fo = fw_off[host_inst.size()];
+                d.flit = fo >= 0 ? flit.as<uint32_t>() + fo : nullptr;
+                d.cs_off = L.cs_off;
+                d.rows_off = L.rows_off;
+            }
             int r;
             if ((r = put(lit, ol, q->lit)) || (r = put(litw, ow, q->litw)) || (r = put(slotw, ow, q->slotw)) ||
                 (r = put(srow, orr, q->srow)) || (r = put(perm, op, q->perm)) ||
@@ -154,6 +182,7 @@ struct Variant {
     int cl;         // CTAs per trajectory (thread-block cluster), global storage only
     SolveFn fn;
     size_t bytes_per_value;
+    bool lean = false;  // solve_kernel_fast: FP32, plain CTDS, offset-carrying literal words
 };
 
 #define AS_VARIANT_F32(K, EX, GS, CL) \
@@ -161,8 +190,12 @@ struct Variant {
 #define AS_VARIANT_F64(K, EX, GS, CL) \
     Variant{AS_PREC_F64, K, EX, GS, CL, &solve_kernel<double, false, K, EX, GS, CL>, 8}
 
+#define AS_VARIANT_LEAN(K) \
+    Variant{AS_PREC_F32_LOGA, K, true, false, 1, &solve_kernel_fast<K>, 4, true}
+
 const std::vector<Variant>& variants() {
     static const std::vector<Variant> v = {
+        AS_VARIANT_LEAN(3), AS_VARIANT_LEAN(4),
         AS_VARIANT_F32(3, true, false, 1),  AS_VARIANT_F32(4, true, false, 1), AS_VARIANT_F32(2, true, false, 1),
         AS_VARIANT_F32(16, false, false, 1), AS_VARIANT_F64(3, true, false, 1), AS_VARIANT_F64(4, true, false, 1),
         AS_VARIANT_F64(16, false, false, 1), AS_VARIANT_F32(3, true, true, 1),  AS_VARIANT_F32(4, true, true, 1),
@@ -174,22 +207,26 @@ const std::vector<Variant>& variants() {
 }
 
 size_t solver_smem(const Variant& v, const PackedProblem& q) {
+    if (v.lean) return fast_layout(q.n, q.m, q.nslots).bytes;
     return solve_smem_values(q.n, q.m, q.nslots) * v.bytes_per_value;
 }
 
 // Shared-memory variants need the compact encoding and the whole trajectory in one
-// SM's shared memory; global-storage variants take any size.
+// SM's shared memory; global-storage variants take any size.  The lean kernel also
+// needs the plain CTDS right-hand side and its byte offsets to fit the literal words.
 bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_limit) {
     const bool kok = v.exact ? q.k == v.kmax : q.k <= v.kmax;
     if (v.precision != precision || !kok) return false;
     if (v.gs) return true;
+    if (v.lean && !(standard_model(q) && fast_layout(q.n, q.m, q.nslots).ok)) return false;
     return q.compact && solver_smem(v, q) <= smem_limit;
 }
 
-// Preference among fitting variants: shared memory first, then exact K, then the
-// smallest KMAX.
+// Preference among fitting variants: the lean kernel, then shared memory, then exact
+// K, then the smallest KMAX.
 long variant_score(const Variant& v) {
-    return (v.gs ? 100000 : 0) + (v.cl > 1 ? 10000 * v.cl : 0) + (v.exact ? 0 : 1000) + v.kmax;
+    return (v.lean ? -100 : 0) + (v.gs ? 100000 : 0) + (v.cl > 1 ? 10000 * v.cl : 0) + (v.exact ? 0 : 1000) +
+           v.kmax;
 }
 
 // CTA size: the smallest clause count per thread (at least 4) that keeps the CTA at
@@ -202,13 +239,13 @@ int preferred_bt(const PackedProblem& q) {
     return std::max(64, std::min(1024, bt));
 }
 
-// CTA size of a shared-memory launch: a trajectory of `vals` shared values that leaves
-// no room for a second CTA on its SM gets the largest CTA (more warps to hide the
-// clause phase's latencies), smaller ones `bt`.
-int shared_cta_threads(size_t vals, size_t bytes_per_value, int bt, int device, int* out) {
+// CTA size of a shared-memory launch: a trajectory of `smem_bytes` that leaves no room
+// for a second CTA on its SM gets the largest CTA (more warps to hide the clause
+// phase's latencies), smaller ones `bt`.
+int shared_cta_threads(size_t smem_bytes, int bt, int device, int* out) {
     int per_sm = 0;
     AS_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
-    *out = 2 * (vals * bytes_per_value + 2048) > (size_t)per_sm ? 1024 : bt;
+    *out = 2 * (smem_bytes + 2048) > (size_t)per_sm ? 1024 : bt;
     return AS_OK;
 }
 
@@ -289,6 +326,7 @@ struct as_solver {
     int track_best = 0;
     int forced_bt = 0;
     int forced_cl = 0;     // CTAs per trajectory in global-storage mode (0 = automatic)
+    int kernel_choice = AS_KERNEL_AUTO;  // AS_KERNEL_GENERIC: never the lean FP32 kernel
     int storage_mode = 0;  // 0 automatic, 1 shared memory, 2 global storage, 3 stream
     std::unique_ptr<StreamPlan> sp;  // streamed solver state
     int stream_parts = 0;            // clause parts per stream pass (0 = from the L2 budget)
@@ -805,6 +843,7 @@ int build_groups(as_solver* s) {
             const auto& v = vs[i];
             if (!fits(v, q, s->precision, s->smem_limit)) continue;
             if ((s->storage_mode == 1 && v.gs) || (s->storage_mode == 2 && !v.gs)) continue;
+            if (v.lean && s->kernel_choice == AS_KERNEL_GENERIC) continue;
             const long score = variant_score(v);
             if (best < 0 || score < best) { best = score; pv[p] = i; }
         }
@@ -861,11 +900,12 @@ int build_groups(as_solver* s) {
         const int vi = pv[pi[s->order[u]]];
         const Variant& v = vs[vi];
         int e = u, bt = 64;
-        size_t vals = 0;
+        size_t vals = 0, sbytes = 0;
         while (e < num_traj && pv[pi[s->order[e]]] == vi) {
             const auto& q = s->problems[pi[s->order[e]]];
             bt = std::max(bt, preferred_bt(q));
             vals = std::max(vals, solve_smem_values(q.n, q.m, q.nslots));
+            sbytes = std::max(sbytes, solver_smem(v, q));
             e++;
         }
         as_solver::Group G;
@@ -884,11 +924,11 @@ int build_groups(as_solver* s) {
         // the largest CTA (more warps to hide the clause phase's latencies)
         int sm_bt = bt;
         if (!v.gs) {
-            const int r = shared_cta_threads(vals, v.bytes_per_value, bt, s->device, &sm_bt);
+            const int r = shared_cta_threads(sbytes, bt, s->device, &sm_bt);
             if (r) return r;
         }
         G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : gs_bt) : sm_bt);
-        G.smem = v.gs ? 0 : vals * v.bytes_per_value;
+        G.smem = v.gs ? 0 : sbytes;
         AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem));
         int occ = 0;
         if (v.cl > 1) {
@@ -1641,6 +1681,16 @@ int32_t as_solver_set_cluster_size(as_solver* s, int32_t ctas) {
     return AS_OK;
 }
 
+int32_t as_solver_set_kernel(as_solver* s, int32_t kernel) {
+    if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
+    if (kernel != AS_KERNEL_AUTO && kernel != AS_KERNEL_GENERIC)
+        return fail(AS_ERR_BAD_INPUT, "as_solver_set_kernel: AS_KERNEL_AUTO or AS_KERNEL_GENERIC");
+    s->kernel_choice = kernel;
+    s->groups_dirty = true;
+    s->invalidate();
+    return AS_OK;
+}
+
 int32_t as_solver_force_threads(as_solver* s, int32_t threads) {
     if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");
     if (threads != 0 && (threads < 32 || threads > 1024 || threads % 32 != 0))
@@ -1747,6 +1797,7 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
     long best = -1;
     for (const auto& cand : variants()) {
         if (cand.gs || !fits(cand, q, s->precision, s->smem_limit)) continue;
+        if (cand.lean && s->kernel_choice == AS_KERNEL_GENERIC) continue;
         const long score = variant_score(cand);
         if (best < 0 || score < best) { best = score; v = &cand; }
     }
@@ -1755,8 +1806,7 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
                                         "memory (only shared-memory launches need no device buffers)");
     int bt = s->forced_bt;
     if (!bt) {
-        r = shared_cta_threads(solve_smem_values(q.n, q.m, q.nslots), v->bytes_per_value,
-                               std::max(64, preferred_bt(q)), s->device, &bt);
+        r = shared_cta_threads(solver_smem(*v, q), std::max(64, preferred_bt(q)), s->device, &bt);
         if (r) return r;
     }
     const size_t smem = solver_smem(*v, q);

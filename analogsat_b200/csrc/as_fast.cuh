@@ -1,0 +1,333 @@
+// Lean FP32 persistent solver (shared-memory mode, plain CTDS right-hand side).
+//
+// The same integrator, counters and early-exit rules as solve_kernel (SatSolver::DoSolve
+// + CpuRungeKutta::Step/rkqs/rkck + CpuSat::GetDerivatives/GetClauseViolationCount:
+// AnalogSAT/solver/SatSolver.h:273-355, AnalogSAT/cpu_sat/CpuRungeKutta.cpp:66-100,
+// 181-267, AnalogSAT/cpu_sat/CpuSat.cpp:65-94,136-173,199-241) and the same FP32
+// arithmetic in the same expression order, with the instruction count per clause cut
+// down -- the shared-memory solver is issue bound, so its RHS rate is the inverse of
+// the instructions it executes per clause and stage:
+//
+//  * Literal words carry shared-memory byte offsets (DevInstance::flit): bits 0-13 the
+//    byte offset of the literal's spin (the spins start at offset 0 of the dynamic
+//    shared memory), bits 14-29 the byte offset of its contribution slot, bit 31 the
+//    sign.  A spin gather is one mask and one load, a contribution store a shift, a
+//    mask and a store: no base-pointer arithmetic.
+//  * Literal words are clause-major (flit[m * K + q]), so a clause's K words are
+//    loads at immediate offsets from one pointer that advances once per clause.
+//  * The six RK vectors of an element are interleaved, [e][X, K1, K2, K3, K4, K5]
+//    (24 bytes per element): a stage input is one row address and 64-bit loads at
+//    immediate offsets (a 16-lane half-warp at a 24-byte stride covers all 32 banks
+//    once, so the pairs load without bank conflicts).  The stage-6 candidate state is
+//    written into K2's place and copied into X's on acceptance (each element by its
+//    own thread, no barrier).
+//  * No model branches: instances with the tanh variant or a bias term use
+//    solve_kernel.
+// The bank-aware clause grouping of the FP32 packing applies unchanged: a literal's
+// spin and its slot both sit in bank (internal variable mod 32).
+#pragma once
+
+#include <type_traits>
+
+#include "as_kernels.cuh"
+
+namespace asb {
+
+// Shared-memory byte offsets of the lean layout for an instance, and whether it
+// qualifies (spin offsets below 16 KB, slot offsets below 64 KB).
+struct FastLayout {
+    bool ok = false;
+    int cs_off = 0, rows_off = 0;
+    size_t bytes = 0;
+};
+__host__ __device__ inline FastLayout fast_layout(int n, int m, int nslots) {
+    FastLayout L;
+    L.cs_off = ((4 * (n + 1)) + 127) / 128 * 128;  // a multiple of 128 B keeps slot banks
+    const long long cs_end = (long long)L.cs_off + 4ll * (nslots + 1);
+    L.rows_off = (int)((cs_end + 15) / 16 * 16);
+    L.bytes = (size_t)L.rows_off + 24ull * (size_t)(n + m);
+    L.ok = 4ll * n < 16384 && (long long)L.cs_off + 4ll * nslots < 65536;
+    return L;
+}
+
+__device__ __forceinline__ uint32_t ld_lit(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::evict_last.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+// Shared-memory access by byte offset from the start of the dynamic shared memory.
+template <typename V>
+__device__ __forceinline__ V& sm_at(unsigned char* base, uint32_t off) {
+    return *reinterpret_cast<V*>(base + off);
+}
+
+// The entries of one element's interleaved row that stage S reads (X, K1..K_{S-1}),
+// in 64-bit loads.
+struct Row6 {
+    float x = 0.f, k1 = 0.f, k2 = 0.f, k3 = 0.f, k4 = 0.f, k5 = 0.f;
+};
+template <int S>
+__device__ __forceinline__ Row6 load_row(const float* r) {
+    Row6 o;
+    if constexpr (S == 1) {
+        o.x = r[0];
+    } else {
+        const float2 a = *reinterpret_cast<const float2*>(r);
+        o.x = a.x; o.k1 = a.y;
+        if constexpr (S == 3) o.k2 = r[2];
+        if constexpr (S >= 4) {
+            const float2 b = *reinterpret_cast<const float2*>(r + 2);
+            o.k2 = b.x; o.k3 = b.y;
+        }
+        if constexpr (S == 5) o.k4 = r[4];
+        if constexpr (S == 6) {
+            const float2 c = *reinterpret_cast<const float2*>(r + 4);
+            o.k4 = c.x; o.k5 = c.y;
+        }
+    }
+    return o;
+}
+template <int S>
+__device__ __forceinline__ float row_input(const Row6& o, float h) {
+    return stage_in<S, float>(o.x, o.k1, o.k2, o.k3, o.k4, o.k5, h);
+}
+
+// 1 - c s for a literal word (the sign bit flips s: 1 - (-s) = 1 + s), as clause_phase.
+__device__ __forceinline__ float lit_factor(unsigned char* sm, uint32_t w) {
+    const float s = sm_at<float>(sm, w & 0x3FFFu);
+    return 1.0f - __int_as_float(__float_as_int(s) ^ (int)(w & 0x80000000u));
+}
+
+// Clause phase of one clause (K literals, FP32, log-space weights): spin gathers,
+// K_m, the leave-one-out products in CpuProdWrapper order, contributions into their
+// slots; returns du_m = K_m^2 / ln 2.  Same operations as clause_phase<float, true, K>.
+template <int K>
+__device__ __forceinline__ float fast_clause(unsigned char* sm, const uint32_t* lp, float am, float knorm) {
+    uint32_t w[K];
+    float f[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) w[q] = ld_lit(lp + q);
+    float km = knorm;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        f[q] = lit_factor(sm, w[q]);
+        km = km * f[q];
+    }
+    const float r = (km * knorm) * am;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        float prod = 1.0f;
+        bool first = true;
+#pragma unroll
+        for (int l = 0; l < K; l++) {
+            if (l != q) {
+                prod = first ? f[l] : prod * f[l];
+                first = false;
+            }
+        }
+        const float rr = (r + r) * prod;  // (2r) prod == 2 (r prod) above the subnormals
+        sm_at<float>(sm, (w[q] >> 14) & 0xFFFFu) = __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u));
+    }
+    return km * km * kInvLn2;
+}
+
+template <int K>
+__global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red_d[36];
+    __shared__ int red_i[33];
+    __shared__ int s_unit, s_flag;
+    const Grp<1> g;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    unsigned char* const sm = smem_raw;
+
+    while (true) {
+        const int u = g.bcast(&s_unit, tid == 0 ? atomicAdd(P.queue_head, 1) : 0);
+        if (u >= P.num_units) break;
+        const int pidx = P.unit_inst[u];
+        if (g.bcast(&s_flag, tid == 0 && P.stop_on_first ? (atomicAdd(P.inst_solved + pidx, 0) != 0 ? 1 : 0) : 0)) {
+            if (tid == 0) {
+                UnitResult r;
+                r.time = 0.0; r.hdid = 0.0; r.status = SAT_ODE_INTERRUPTED; r.steps = 0; r.attempts = 0;
+                r.rhs = 0; r.viol = -1; r.min_viol = -1;
+                r.pad0 = r.pad1 = 0;
+                P.results[u] = r;
+            }
+            g.sync();
+            continue;
+        }
+        const DevInstance I = P.inst[pidx];
+        const int n = I.n, m = I.m;
+        float* const sy = reinterpret_cast<float*>(sm);
+        float* const cs = reinterpret_cast<float*>(sm + I.cs_off);
+        float* const rows = reinterpret_cast<float*>(sm + I.rows_off);
+        float* G = reinterpret_cast<float*>(P.states) + P.unit_state[u];
+        const float knorm = (float)ldexp(1.0, -I.k);
+
+        // initial state: public spins to internal order, a -> log2 a
+        for (int i = tid; i < n; i += nt) rows[6 * __ldg(I.iperm + i)] = G[i];
+        for (int j = tid; j < m; j += nt) rows[6 * (n + __ldg(I.icperm + j))] = log2f(G[n + j]);
+        for (int j = tid; j <= I.nslots; j += nt) cs[j] = 0.0f;
+        if (tid == 0) sy[n] = -1.0f;  // sentinel spin: padding literals are always FALSE
+        g.sync();  // the scatter above wrote rows that other threads own in the stage loops
+
+        // One RHS evaluation at stage S (the stage input formed from the rows); the
+        // derivative lands in slot S of the rows, or for S == 6 is consumed at once into
+        // the candidate state (slot 2) and the error norm.
+        auto eval = [&](auto stage, float hT, float h0T, float& em) {
+            constexpr int S = decltype(stage)::value;
+            for (int v = tid; v < n; v += nt) sy[v] = row_input<S>(load_row<S>(rows + 6 * v), hT);
+            g.sync();
+            const uint32_t* lp = I.flit + (size_t)tid * K;
+            for (int c = tid; c < m; c += nt, lp += (size_t)nt * K) {
+                float* r = rows + 6 * (n + c);
+                const Row6 o = load_row<S>(r);
+                const float d = fast_clause<K>(sm, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+                if constexpr (S < 6) {
+                    r[S] = d;
+                } else {
+                    em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, d, hT, h0T, true));
+                    r[2] = rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT);
+                }
+            }
+            g.sync();
+            for (int v = tid; v < n; v += nt) {
+                const int g32 = v >> 5;
+                const int r0 = ld_ro(I.srow + g32), r1 = ld_ro(I.srow + g32 + 1);
+                const float* p = cs + r0 * 32 + (v & 31);
+                float sum = 0.0f;
+#pragma unroll 4
+                for (int k = r0; k < r1; k++, p += 32) sum = sum + *p;
+                float* r = rows + 6 * v;
+                if constexpr (S < 6) {
+                    r[S] = sum;
+                } else {
+                    const float x = r[0], k1 = r[1], k3 = r[3], k4 = r[4], k5 = r[5];
+                    em = fmaxf(em, rk_err_ratio(x, k1, k3, k4, k5, sum, hT, h0T, false));
+                    r[2] = rk_new<float>(x, k1, k3, k4, sum, hT);
+                }
+            }
+        };
+
+        double t = 0.0, hnext = 1e-9, hdid = 0.0;
+        int steps = 0, attempts = 0, rhs = 0, viol = -1, minviol = INT_MAX;
+        int status = SAT_UNKNOWN;
+
+        while (status == SAT_UNKNOWN && t < P.tmax && steps < P.maxsteps) {
+            bool underflow = false, interrupted = false;
+            int taken = 0;
+            for (int b = 0; b < P.batch; b++) {
+                float dummy = 0.0f;
+                eval(std::integral_constant<int, 1>{}, 0.0f, 0.0f, dummy);
+                rhs++;
+                const double h0 = hnext;
+                const float h0T = (float)h0;
+                double h = hnext, ermax = 0.0;
+                while (true) {
+                    const float hT = (float)h;
+                    float em = 0.0f;
+                    eval(std::integral_constant<int, 2>{}, hT, h0T, em);
+                    eval(std::integral_constant<int, 3>{}, hT, h0T, em);
+                    eval(std::integral_constant<int, 4>{}, hT, h0T, em);
+                    eval(std::integral_constant<int, 5>{}, hT, h0T, em);
+                    eval(std::integral_constant<int, 6>{}, hT, h0T, em);
+                    rhs += 5;
+                    attempts++;
+                    ermax = group_max_then<1>(g, (double)em, red_d, [&](double emax) {
+                        const double e = __ddiv_rn(emax, P.eps);
+                        double hn;
+                        if (e <= 1.0)
+                            hn = e > ck::ERRCON ? __dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PGROW))
+                                                : __dmul_rn(5.0, h);
+                        else
+                            hn = fmax(__dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PSHRNK)),
+                                      __dmul_rn(ck::HFACTOR, h));
+                        red_d[34] = hn;
+                        const bool quit = (P.stop_on_first && atomicAdd(P.inst_solved + pidx, 0) != 0) ||
+                                          (P.deadline && globaltimer_ns() >= *P.deadline);
+                        red_d[35] = quit ? 1.0 : 0.0;
+                        return e;
+                    });
+                    const double hn = red_d[34];
+                    if (red_d[35] != 0.0) { interrupted = true; break; }
+                    if (ermax <= 1.0) { hnext = hn; break; }
+                    h = hn;
+                    if (__dadd_rn(t, h) == t) { underflow = true; break; }
+                }
+                if (underflow || interrupted) break;
+                hdid = h;
+                t = __dadd_rn(t, h);
+                taken++;
+                // accept: the candidate state (slot 2) becomes the state, each element by
+                // the thread that owns it in the stage loops
+                for (int v = tid; v < n; v += nt) rows[6 * v] = rows[6 * v + 2];
+                for (int c = tid; c < m; c += nt) rows[6 * (n + c)] = rows[6 * (n + c) + 2];
+            }
+            if (underflow) { status = SAT_UNDERFLOW; break; }
+            steps += taken;
+            if (interrupted) { status = SAT_ODE_INTERRUPTED; break; }
+
+            // CpuSat::GetClauseViolationCount on the accepted state
+            for (int v = tid; v < n; v += nt) sy[v] = rows[6 * v];
+            g.sync();
+            int cnt = 0;
+            {
+                const uint32_t* lp = I.flit + (size_t)tid * K;
+                for (int c = tid; c < m; c += nt, lp += (size_t)nt * K) {
+                    bool sat = false;
+#pragma unroll
+                    for (int q = 0; q < K; q++) {
+                        const uint32_t w = ld_lit(lp + q);
+                        const bool tv = sm_at<float>(sm, w & 0x3FFFu) > 0.0f;
+                        sat |= (w & 0x80000000u) ? !tv : tv;
+                    }
+                    cnt += sat ? 0 : 1;
+                }
+            }
+            viol = group_sum<1>(g, cnt, red_i);
+            if (viol < minviol) {
+                minviol = viol;
+                if (P.best_bits) {
+                    uint32_t* bits = P.best_bits + P.unit_bits[u];
+                    for (int i0 = tid & ~31; i0 < n; i0 += nt) {
+                        const int i = i0 + (tid & 31);
+                        const bool bb = i < n && sy[__ldg(I.iperm + (i < n ? i : 0))] > 0.0f;
+                        const unsigned bal = __ballot_sync(0xffffffffu, bb);
+                        if ((tid & 31) == 0) bits[i0 >> 5] = bal;
+                    }
+                }
+            }
+            if (viol == 0) {
+                status = SAT_SOLUTION_FOUND;
+                if (tid == 0 && P.stop_on_first) atomicExch(P.inst_solved + pidx, 1);
+                break;
+            }
+            int f = 0;
+            if (tid == 0) {
+                if (P.deadline && globaltimer_ns() >= *P.deadline) f = 1;
+                if (P.stop_on_first && atomicAdd(P.inst_solved + pidx, 0) != 0) f = 1;
+            }
+            if (g.bcast(&s_flag, f)) { status = SAT_ODE_INTERRUPTED; break; }
+        }
+        if (status == SAT_UNKNOWN) {
+            if (t >= P.tmax) status = SAT_MAXTIME_REACHED;
+            else if (steps >= P.maxsteps) status = SAT_MAXITER_REACHED;
+        }
+
+        // write back the final state in the public layout
+        g.sync();
+        for (int i = tid; i < n; i += nt) G[i] = rows[6 * __ldg(I.iperm + i)];
+        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(rows[6 * (n + __ldg(I.icperm + j))]);
+        if (tid == 0) {
+            UnitResult r;
+            r.time = t; r.hdid = hdid; r.status = status; r.steps = steps; r.attempts = attempts;
+            r.rhs = rhs; r.viol = viol; r.min_viol = minviol == INT_MAX ? -1 : minviol;
+            r.pad0 = r.pad1 = 0;
+            P.results[u] = r;
+        }
+        g.sync();
+    }
+}
+
+}  // namespace asb

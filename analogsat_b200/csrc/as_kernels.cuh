@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel(SolveParams P) {
         }
         for (int j = tid; j <= I.nslots; j += nt) cs[j] = T(0);
         if (tid == 0) sy[n] = T(-1);  // sentinel spin: padding literals are always FALSE
+        g.sync();  // the scatter above wrote elements that other threads own in the stage loops
 
         double t = 0.0, hnext = 1e-9, hdid = 0.0;
         int steps = 0, attempts = 0, rhs = 0, viol = -1, minviol = INT_MAX;

@@ -258,6 +258,16 @@ int32_t as_solver_get_launch_shape(as_solver* s, int32_t* threads, int32_t* ctas
  * the automatic choice (the fewest threads that give every thread about the same
  * clause count, at least four).  Used by the autotuner. */
 int32_t as_solver_force_threads(as_solver* s, int32_t threads);
+/* Solver kernel of the shared-memory mode (no reference counterpart).  AS_KERNEL_AUTO
+ * (default) runs FP32 instances with the plain CTDS right-hand side (no tanh variant,
+ * no bias term), clause length 3 or 4 and N < 4096 on the lean kernel, whose literal
+ * words carry shared-memory byte offsets and whose RK vectors are interleaved per
+ * element: the same integrator and arithmetic with fewer instructions per clause.
+ * AS_KERNEL_GENERIC keeps every instance on the general kernel.  Results of the two
+ * agree to FP32 rounding. */
+#define AS_KERNEL_AUTO 0
+#define AS_KERNEL_GENERIC 1
+int32_t as_solver_set_kernel(as_solver* s, int32_t kernel);
 /* Where a trajectory lives while it is integrated (no reference counterpart):
  * AS_STORAGE_AUTO picks the streamed solver when every instance has N + M >= 2^19
  * state elements, else shared memory when the instance fits one SM, else global

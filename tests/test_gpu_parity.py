@@ -357,3 +357,31 @@ def test_result_file_and_perf_line(golden, tmp_path):
     assert len(rows) == 2 and all(len(rw) == 7 for rw in rows)
     assert rows[0][0] == "p50" and rows[0][3] == "solution found"
     assert int(rows[0][6]) == r["rhs"][0] and float(rows[0][4]) > 0
+
+
+@pytest.mark.parametrize("tag", ["p50", "r4", "p200", "p1000"])
+def test_lean_kernel_matches_generic_kernel(golden, tag):
+    """The lean FP32 kernel (literal words carrying shared-memory byte offsets,
+    interleaved RK rows; as_solver_set_kernel) runs the general FP32 kernel's
+    integrator and arithmetic: over 8 trajectories and 300 steps the same accepted and
+    attempted steps and RHS counts, and states equal to FP32 rounding (relative 1e-6).
+    The two launch plans differ (the lean layout's shared-memory size), which shows
+    that each kernel ran."""
+    from analogsat_b200 import AS_PREC_F32_LOGA, _abi
+    n, m, _ = (int(v) for v in golden[f"{tag}/nmk"])
+    from analogsat_b200.instances import initial_states
+    ics = initial_states(n, m, 8, seed=77, dtype=np.float32)
+    out, shapes = {}, {}
+    for kern in (_abi.AS_KERNEL_GENERIC, _abi.AS_KERNEL_AUTO):
+        s = _solver(golden, tag, AS_PREC_F32_LOGA, 1e-6, 25, 300)
+        s.SetKernel(kern)
+        s.SetSatStates(np.zeros(8, np.int32), ics)
+        s.Solve()
+        out[kern] = (s.results(), s.GetSatStates(np.float32).reshape(8, -1))
+        shapes[kern] = s.launch_shape()["smem_bytes"]
+    (ra, xa), (rb, xb) = out[_abi.AS_KERNEL_GENERIC], out[_abi.AS_KERNEL_AUTO]
+    assert shapes[_abi.AS_KERNEL_GENERIC] != shapes[_abi.AS_KERNEL_AUTO]
+    for key in ("status", "steps", "attempts", "rhs", "violations"):
+        assert np.array_equal(ra[key], rb[key]), key
+    np.testing.assert_allclose(xb, xa, rtol=1e-6, atol=1e-6)
+    print(tag, "bit-identical" if np.array_equal(xa, xb) else f"max diff {np.abs(xa - xb).max():.3g}")
