@@ -225,8 +225,8 @@ bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_l
 // Preference among fitting variants: the lean kernel, then shared memory, then exact
 // K, then the smallest KMAX.
 long variant_score(const Variant& v) {
-    return (v.lean ? -100 : 0) + (v.gs ? 100000 : 0) + (v.cl > 1 ? 10000 * v.cl : 0) + (v.exact ? 0 : 1000) +
-           v.kmax;
+    return (v.gs ? 100000 : 0) + (v.cl > 1 ? 10000 * v.cl : 0) + (v.exact ? 0 : 1000) + 2 * v.kmax +
+           (v.lean ? 0 : 1);
 }
 
 // CTA size: the smallest clause count per thread (at least 4) that keeps the CTA at
@@ -845,7 +845,7 @@ int build_groups(as_solver* s) {
             if ((s->storage_mode == 1 && v.gs) || (s->storage_mode == 2 && !v.gs)) continue;
             if (v.lean && s->kernel_choice == AS_KERNEL_GENERIC) continue;
             const long score = variant_score(v);
-            if (best < 0 || score < best) { best = score; pv[p] = i; }
+            if (pv[p] < 0 || score < best) { best = score; pv[p] = i; }
         }
         if (pv[p] < 0)
             return fail(AS_ERR_UNSUPPORTED, "no compiled launch shape fits problem " + std::to_string(p));
@@ -1799,7 +1799,7 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
         if (cand.gs || !fits(cand, q, s->precision, s->smem_limit)) continue;
         if (cand.lean && s->kernel_choice == AS_KERNEL_GENERIC) continue;
         const long score = variant_score(cand);
-        if (best < 0 || score < best) { best = score; v = &cand; }
+        if (!v || score < best) { best = score; v = &cand; }
     }
     if (!v)
         return fail(AS_ERR_UNSUPPORTED, "as_solver_solve_noalloc: the instance does not fit one SM's shared "
