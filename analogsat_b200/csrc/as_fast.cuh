@@ -56,10 +56,20 @@ __device__ __forceinline__ uint32_t ld_lit(const uint32_t* p) {
     return v;
 }
 
-// Shared-memory access by byte offset from the start of the dynamic shared memory.
-template <typename V>
-__device__ __forceinline__ V& sm_at(unsigned char* base, uint32_t off) {
-    return *reinterpret_cast<V*>(base + off);
+// Shared-memory accesses by 32-bit shared-window address (the dynamic shared memory's
+// base plus a byte offset), so no address arithmetic is wider than 32 bits.
+__device__ __forceinline__ float lds(uint32_t a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float2 lds2(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void sts(uint32_t a, float v) {
+    asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
 }
 
 // The entries of one element's interleaved row that stage S reads (X, K1..K_{S-1}),
@@ -68,21 +78,21 @@ struct Row6 {
     float x = 0.f, k1 = 0.f, k2 = 0.f, k3 = 0.f, k4 = 0.f, k5 = 0.f;
 };
 template <int S>
-__device__ __forceinline__ Row6 load_row(const float* r) {
+__device__ __forceinline__ Row6 load_row(uint32_t r) {
     Row6 o;
     if constexpr (S == 1) {
-        o.x = r[0];
+        o.x = lds(r);
     } else {
-        const float2 a = *reinterpret_cast<const float2*>(r);
+        const float2 a = lds2(r);
         o.x = a.x; o.k1 = a.y;
-        if constexpr (S == 3) o.k2 = r[2];
+        if constexpr (S == 3) o.k2 = lds(r + 8);
         if constexpr (S >= 4) {
-            const float2 b = *reinterpret_cast<const float2*>(r + 2);
+            const float2 b = lds2(r + 8);
             o.k2 = b.x; o.k3 = b.y;
         }
-        if constexpr (S == 5) o.k4 = r[4];
+        if constexpr (S == 5) o.k4 = lds(r + 16);
         if constexpr (S == 6) {
-            const float2 c = *reinterpret_cast<const float2*>(r + 4);
+            const float2 c = lds2(r + 16);
             o.k4 = c.x; o.k5 = c.y;
         }
     }
@@ -94,8 +104,8 @@ __device__ __forceinline__ float row_input(const Row6& o, float h) {
 }
 
 // 1 - c s for a literal word (the sign bit flips s: 1 - (-s) = 1 + s), as clause_phase.
-__device__ __forceinline__ float lit_factor(unsigned char* sm, uint32_t w) {
-    const float s = sm_at<float>(sm, w & 0x3FFFu);
+__device__ __forceinline__ float lit_factor(uint32_t sm0, uint32_t w) {
+    const float s = lds(sm0 + (w & 0x3FFFu));
     return 1.0f - __int_as_float(__float_as_int(s) ^ (int)(w & 0x80000000u));
 }
 
@@ -103,7 +113,7 @@ __device__ __forceinline__ float lit_factor(unsigned char* sm, uint32_t w) {
 // K_m, the leave-one-out products in CpuProdWrapper order, contributions into their
 // slots; returns du_m = K_m^2 / ln 2.  Same operations as clause_phase<float, true, K>.
 template <int K>
-__device__ __forceinline__ float fast_clause(unsigned char* sm, const uint32_t* lp, float am, float knorm) {
+__device__ __forceinline__ float fast_clause(uint32_t sm0, const uint32_t* lp, float am, float knorm) {
     uint32_t w[K];
     float f[K];
 #pragma unroll
@@ -111,7 +121,7 @@ __device__ __forceinline__ float fast_clause(unsigned char* sm, const uint32_t* 
     float km = knorm;
 #pragma unroll
     for (int q = 0; q < K; q++) {
-        f[q] = lit_factor(sm, w[q]);
+        f[q] = lit_factor(sm0, w[q]);
         km = km * f[q];
     }
     const float r = (km * knorm) * am;
@@ -127,7 +137,7 @@ __device__ __forceinline__ float fast_clause(unsigned char* sm, const uint32_t* 
             }
         }
         const float rr = (r + r) * prod;  // (2r) prod == 2 (r prod) above the subnormals
-        sm_at<float>(sm, (w[q] >> 14) & 0xFFFFu) = __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u));
+        sts(sm0 + ((w[q] >> 14) & 0xFFFFu), __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u)));
     }
     return km * km * kInvLn2;
 }
@@ -140,7 +150,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
     __shared__ int s_unit, s_flag;
     const Grp<1> g;
     const int tid = threadIdx.x, nt = blockDim.x;
-    unsigned char* const sm = smem_raw;
+    const uint32_t sm0 = (uint32_t)__cvta_generic_to_shared(smem_raw);
 
     while (true) {
         const int u = g.bcast(&s_unit, tid == 0 ? atomicAdd(P.queue_head, 1) : 0);
@@ -159,9 +169,11 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         }
         const DevInstance I = P.inst[pidx];
         const int n = I.n, m = I.m;
-        float* const sy = reinterpret_cast<float*>(sm);
-        float* const cs = reinterpret_cast<float*>(sm + I.cs_off);
-        float* const rows = reinterpret_cast<float*>(sm + I.rows_off);
+        float* const sy = reinterpret_cast<float*>(smem_raw);
+        float* const cs = reinterpret_cast<float*>(smem_raw + I.cs_off);
+        float* const rows = reinterpret_cast<float*>(smem_raw + I.rows_off);
+        const uint32_t rows0 = sm0 + (uint32_t)I.rows_off;  // row e at rows0 + 24 e
+        const uint32_t cs0 = sm0 + (uint32_t)I.cs_off;
         float* G = reinterpret_cast<float*>(P.states) + P.unit_state[u];
         const float knorm = (float)ldexp(1.0, -I.k);
 
@@ -177,35 +189,36 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         // the candidate state (slot 2) and the error norm.
         auto eval = [&](auto stage, float hT, float h0T, float& em) {
             constexpr int S = decltype(stage)::value;
-            for (int v = tid; v < n; v += nt) sy[v] = row_input<S>(load_row<S>(rows + 6 * v), hT);
+            for (int v = tid; v < n; v += nt)
+                sts(sm0 + 4u * (uint32_t)v, row_input<S>(load_row<S>(rows0 + 24u * (uint32_t)v), hT));
             g.sync();
             const uint32_t* lp = I.flit + (size_t)tid * K;
-            for (int c = tid; c < m; c += nt, lp += (size_t)nt * K) {
-                float* r = rows + 6 * (n + c);
-                const Row6 o = load_row<S>(r);
-                const float d = fast_clause<K>(sm, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+            uint32_t ra = rows0 + 24u * (uint32_t)(n + tid);
+            for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra += 24u * (uint32_t)nt) {
+                const Row6 o = load_row<S>(ra);
+                const float d = fast_clause<K>(sm0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
                 if constexpr (S < 6) {
-                    r[S] = d;
+                    sts(ra + 4u * S, d);
                 } else {
                     em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, d, hT, h0T, true));
-                    r[2] = rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT);
+                    sts(ra + 8u, rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT));
                 }
             }
             g.sync();
             for (int v = tid; v < n; v += nt) {
                 const int g32 = v >> 5;
                 const int r0 = ld_ro(I.srow + g32), r1 = ld_ro(I.srow + g32 + 1);
-                const float* p = cs + r0 * 32 + (v & 31);
+                uint32_t p = cs0 + 4u * (uint32_t)(r0 * 32 + (v & 31));
                 float sum = 0.0f;
 #pragma unroll 4
-                for (int k = r0; k < r1; k++, p += 32) sum = sum + *p;
-                float* r = rows + 6 * v;
+                for (int k = r0; k < r1; k++, p += 128u) sum = sum + lds(p);
+                const uint32_t r = rows0 + 24u * (uint32_t)v;
                 if constexpr (S < 6) {
-                    r[S] = sum;
+                    sts(r + 4u * S, sum);
                 } else {
-                    const float x = r[0], k1 = r[1], k3 = r[3], k4 = r[4], k5 = r[5];
-                    em = fmaxf(em, rk_err_ratio(x, k1, k3, k4, k5, sum, hT, h0T, false));
-                    r[2] = rk_new<float>(x, k1, k3, k4, sum, hT);
+                    const Row6 o = load_row<6>(r);
+                    em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
+                    sts(r + 8u, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
                 }
             }
         };
@@ -261,15 +274,21 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 taken++;
                 // accept: the candidate state (slot 2) becomes the state, each element by
                 // the thread that owns it in the stage loops
-                for (int v = tid; v < n; v += nt) rows[6 * v] = rows[6 * v + 2];
-                for (int c = tid; c < m; c += nt) rows[6 * (n + c)] = rows[6 * (n + c) + 2];
+                for (int v = tid; v < n; v += nt) {
+                    const uint32_t r = rows0 + 24u * (uint32_t)v;
+                    sts(r, lds(r + 8u));
+                }
+                for (int c = tid; c < m; c += nt) {
+                    const uint32_t r = rows0 + 24u * (uint32_t)(n + c);
+                    sts(r, lds(r + 8u));
+                }
             }
             if (underflow) { status = SAT_UNDERFLOW; break; }
             steps += taken;
             if (interrupted) { status = SAT_ODE_INTERRUPTED; break; }
 
             // CpuSat::GetClauseViolationCount on the accepted state
-            for (int v = tid; v < n; v += nt) sy[v] = rows[6 * v];
+            for (int v = tid; v < n; v += nt) sts(sm0 + 4u * (uint32_t)v, lds(rows0 + 24u * (uint32_t)v));
             g.sync();
             int cnt = 0;
             {
@@ -279,7 +298,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
 #pragma unroll
                     for (int q = 0; q < K; q++) {
                         const uint32_t w = ld_lit(lp + q);
-                        const bool tv = sm_at<float>(sm, w & 0x3FFFu) > 0.0f;
+                        const bool tv = lds(sm0 + (w & 0x3FFFu)) > 0.0f;
                         sat |= (w & 0x80000000u) ? !tv : tv;
                     }
                     cnt += sat ? 0 : 1;
