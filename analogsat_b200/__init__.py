@@ -418,6 +418,10 @@ class SatSolver:
         return dict(loss=loss, grad_x0=gx, grad_w=gw[: sum(ms)], nsteps=ns,
                     step_sizes=[hs[t, : ns[t]].copy() for t in range(nt)])
 
+    def kernel_name(self) -> str:
+        """Solver kernel of the last solve's final launch group."""
+        return self._lib.as_solver_kernel_name(self._h).decode()
+
     def launch_shape(self) -> dict:
         a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
         check(self._lib.as_solver_get_launch_shape(self._h, C.byref(a), C.byref(b), C.byref(c),

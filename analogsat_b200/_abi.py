@@ -83,6 +83,7 @@ SIGNATURES = [
     ("as_solver_get_launch_shape", _i32, [_vp, _pi32, _pi32, _pi32, _pi32]),
     ("as_solver_force_threads", _i32, [_vp, _i32]),
     ("as_solver_set_kernel", _i32, [_vp, _i32]),
+    ("as_solver_kernel_name", C.c_char_p, [_vp]),
     ("as_solver_set_storage_mode", _i32, [_vp, _i32]),
     ("as_solver_set_cluster_size", _i32, [_vp, _i32]),
     ("as_solver_set_stream_parts", _i32, [_vp, _i32]),

@@ -183,6 +183,7 @@ struct Variant {
     SolveFn fn;
     size_t bytes_per_value;
     bool lean = false;  // solve_kernel_fast: FP32, plain CTDS, offset-carrying literal words
+    const char* name() const { return lean ? "solve_kernel_fast" : "solve_kernel"; }
 };
 
 #define AS_VARIANT_F32(K, EX, GS, CL) \
@@ -352,6 +353,7 @@ struct as_solver {
     bool graph_valid = false;
     bool groups_dirty = true;
     int last_bt = 0, last_ctas = 0, last_smem = 0, last_occ = 0;
+    const char* last_kernel = "";
 
     ~as_solver() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1058,6 +1060,7 @@ int record_solve(as_solver* s, cudaStream_t st) {
             AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(G.bt), args, smem, st));
         }
         s->last_bt = G.bt; s->last_ctas = ctas; s->last_smem = (int)smem; s->last_occ = occ;
+        s->last_kernel = v.name();
     }
     return AS_OK;
 }
@@ -1300,6 +1303,7 @@ int stream_record_pass(as_solver* s, cudaStream_t st, const unsigned long long* 
         const int pc = std::max(1, std::min((m + BT - 1) / BT, sms * 8));
         stream_post_kernel<T, KMAX, EXACT><<<pv + pc + nbw, BT, 0, st>>>(A, pv, pc);
         s->last_bt = BT;
+        s->last_kernel = "stream_clause_kernel+stream_var_kernel";
         s->last_ctas = gc;
         s->last_smem = 0;
         s->last_occ = 0;
@@ -1680,6 +1684,8 @@ int32_t as_solver_set_cluster_size(as_solver* s, int32_t ctas) {
     s->invalidate();
     return AS_OK;
 }
+
+const char* as_solver_kernel_name(const as_solver* s) { return s ? s->last_kernel : ""; }
 
 int32_t as_solver_set_kernel(as_solver* s, int32_t kernel) {
     if (!s) return fail(AS_ERR_BAD_INPUT, "null solver");

@@ -453,12 +453,12 @@ def run_ours(args):
         else "first solution per instance stops its other trajectories",
         "gpu_launches": args.steps * len(solver_groups(solver)),
         "launch_shape": dict(solver.launch_shape(), autotuned=shape is not None and not args.threads),
-        "roofline": {"bound": "hbm", "kernel": "solve_kernel", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": solver.kernel_name(), "achieved": achieved,
                      "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                     # ncu dram__bytes_read+write of one solve_kernel launch over 148
-                     # trajectories (profiles/solve_kernel_planted3sat_N1000_M4250.md):
-                     # 3.30 MB, i.e. 22.3 KB per trajectory, scaled to this launch
-                     "traffic": 3.298e6 / 148 * len(pidx),
+                     # ncu dram__bytes_read+write of one solve_kernel_fast launch over 148
+                     # trajectories (profiles/solve_kernel_fast_planted3sat_N1000_M4250.md):
+                     # 3.29 MB, i.e. 22.3 KB per trajectory, scaled to this launch
+                     "traffic": 3.294e6 / 148 * len(pidx),
                      "note": "achieved = RHS evals x 8(N+M)+4KM bytes / kernel time; state, "
                              "stages and contributions stay on chip (shared memory), so DRAM "
                              "traffic is far below the algorithmic bytes"},

@@ -268,6 +268,9 @@ int32_t as_solver_force_threads(as_solver* s, int32_t threads);
 #define AS_KERNEL_AUTO 0
 #define AS_KERNEL_GENERIC 1
 int32_t as_solver_set_kernel(as_solver* s, int32_t kernel);
+/* Name of the solver kernel of the last solve's final launch group ("" before the
+ * first solve; no reference counterpart). */
+const char* as_solver_kernel_name(const as_solver* s);
 /* Where a trajectory lives while it is integrated (no reference counterpart):
  * AS_STORAGE_AUTO picks the streamed solver when every instance has N + M >= 2^19
  * state elements, else shared memory when the instance fits one SM, else global

@@ -378,9 +378,11 @@ def test_lean_kernel_matches_generic_kernel(golden, tag):
         s.SetSatStates(np.zeros(8, np.int32), ics)
         s.Solve()
         out[kern] = (s.results(), s.GetSatStates(np.float32).reshape(8, -1))
-        shapes[kern] = s.launch_shape()["smem_bytes"]
+        shapes[kern] = (s.launch_shape()["smem_bytes"], s.kernel_name())
     (ra, xa), (rb, xb) = out[_abi.AS_KERNEL_GENERIC], out[_abi.AS_KERNEL_AUTO]
-    assert shapes[_abi.AS_KERNEL_GENERIC] != shapes[_abi.AS_KERNEL_AUTO]
+    assert shapes[_abi.AS_KERNEL_GENERIC][0] != shapes[_abi.AS_KERNEL_AUTO][0]
+    assert shapes[_abi.AS_KERNEL_GENERIC][1] == "solve_kernel"
+    assert shapes[_abi.AS_KERNEL_AUTO][1] == "solve_kernel_fast"
     for key in ("status", "steps", "attempts", "rhs", "violations"):
         assert np.array_equal(ra[key], rb[key]), key
     np.testing.assert_allclose(xb, xa, rtol=1e-6, atol=1e-6)
