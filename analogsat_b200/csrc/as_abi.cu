@@ -95,8 +95,9 @@ struct DevicePool {
         AS_CUDA(icperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(cperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
-        // clause-major literal words with shared-memory byte offsets for the lean FP32
-        // solver, for the instances whose offsets fit (bits 0-13 spin, 14-29 slot, 31 sign)
+        // clause-major literal words with shared-memory addressing for the lean FP32
+        // solver, for the instances that fit (bits 0-13 spin byte offset, 14-30 slot
+        // index, 31 sign)
         std::vector<uint32_t> fw;
         std::vector<long long> fw_off;
         for (auto* q : pk) {
@@ -110,7 +111,7 @@ struct DevicePool {
                 for (int qq = 0; qq < q->k; qq++) {
                     const uint32_t w = q->lit[(size_t)qq * q->mp + c];
                     const uint32_t var = (w >> 16) & 0x7fffu, slot = w & 0xffffu;
-                    fw.push_back((w & 0x80000000u) | (((uint32_t)L.cs_off + 4u * slot) << 14) | (4u * var));
+                    fw.push_back((w & 0x80000000u) | (slot << 14) | (4u * var));
                 }
         }
         AS_CUDA(flit.alloc(std::max<size_t>(fw.size(), 1) * 4));
@@ -192,11 +193,13 @@ struct Variant {
     Variant{AS_PREC_F64, K, EX, GS, CL, &solve_kernel<double, false, K, EX, GS, CL>, 8}
 
 #define AS_VARIANT_LEAN(K) \
-    Variant{AS_PREC_F32_LOGA, K, true, false, 1, &solve_kernel_fast<K>, 4, true}
+    Variant{AS_PREC_F32_LOGA, K, true, false, 1, &solve_kernel_fast<K, false>, 4, true}
+#define AS_VARIANT_LEAN_G(K) \
+    Variant{AS_PREC_F32_LOGA, K, true, true, 1, &solve_kernel_fast<K, true>, 4, true}
 
 const std::vector<Variant>& variants() {
     static const std::vector<Variant> v = {
-        AS_VARIANT_LEAN(3), AS_VARIANT_LEAN(4),
+        AS_VARIANT_LEAN(3), AS_VARIANT_LEAN(4), AS_VARIANT_LEAN_G(3), AS_VARIANT_LEAN_G(4),
         AS_VARIANT_F32(3, true, false, 1),  AS_VARIANT_F32(4, true, false, 1), AS_VARIANT_F32(2, true, false, 1),
         AS_VARIANT_F32(16, false, false, 1), AS_VARIANT_F64(3, true, false, 1), AS_VARIANT_F64(4, true, false, 1),
         AS_VARIANT_F64(16, false, false, 1), AS_VARIANT_F32(3, true, true, 1),  AS_VARIANT_F32(4, true, true, 1),
@@ -208,8 +211,19 @@ const std::vector<Variant>& variants() {
 }
 
 size_t solver_smem(const Variant& v, const PackedProblem& q) {
-    if (v.lean) return fast_layout(q.n, q.m, q.nslots).bytes;
+    if (v.lean) {
+        const FastLayout L = fast_layout(q.n, q.m, q.nslots);
+        return v.gs ? L.bytes_g : L.bytes;
+    }
+    if (v.gs) return 0;
     return solve_smem_values(q.n, q.m, q.nslots) * v.bytes_per_value;
+}
+
+// Values of a trajectory's per-CTA global slab (global-storage variants).
+size_t solver_slab_values(const Variant& v, const PackedProblem& q) {
+    if (!v.gs) return 0;
+    if (v.lean) return 6 * (size_t)(q.n + q.m);  // the interleaved RK rows
+    return solve_smem_values(q.n, q.m, q.nslots);
 }
 
 // Shared-memory variants need the compact encoding and the whole trajectory in one
@@ -218,16 +232,19 @@ size_t solver_smem(const Variant& v, const PackedProblem& q) {
 bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_limit) {
     const bool kok = v.exact ? q.k == v.kmax : q.k <= v.kmax;
     if (v.precision != precision || !kok) return false;
+    if (v.lean) return standard_model(q) && q.compact && fast_layout(q.n, q.m, q.nslots).ok &&
+                       solver_smem(v, q) <= smem_limit;
     if (v.gs) return true;
-    if (v.lean && !(standard_model(q) && fast_layout(q.n, q.m, q.nslots).ok)) return false;
     return q.compact && solver_smem(v, q) <= smem_limit;
 }
 
 // Preference among fitting variants: the lean kernel, then shared memory, then exact
 // K, then the smallest KMAX.
 long variant_score(const Variant& v) {
-    return (v.gs ? 100000 : 0) + (v.cl > 1 ? 10000 * v.cl : 0) + (v.exact ? 0 : 1000) + 2 * v.kmax +
-           (v.lean ? 0 : 1);
+    // the lean kernel with its rows in global memory still gathers and scatters in
+    // shared memory: after every all-shared variant, before the general global one
+    const long storage = v.gs ? (v.lean ? 50000 : 100000) : 0;
+    return storage + (v.cl > 1 ? 10000 * v.cl : 0) + (v.exact ? 0 : 1000) + 2 * v.kmax + (v.lean ? 0 : 1);
 }
 
 // CTA size: the smallest clause count per thread (at least 4) that keeps the CTA at
@@ -906,7 +923,7 @@ int build_groups(as_solver* s) {
         while (e < num_traj && pv[pi[s->order[e]]] == vi) {
             const auto& q = s->problems[pi[s->order[e]]];
             bt = std::max(bt, preferred_bt(q));
-            vals = std::max(vals, solve_smem_values(q.n, q.m, q.nslots));
+            vals = std::max(vals, solver_slab_values(v, q));
             sbytes = std::max(sbytes, solver_smem(v, q));
             e++;
         }
@@ -917,7 +934,7 @@ int build_groups(as_solver* s) {
         // global storage: 512 threads (two CTAs per SM) while the in-flight slabs fit in
         // L2, else 1,024 (one per SM, half the slabs)
         int gs_bt = 512;
-        if (v.gs && v.cl == 1) {
+        if (v.gs && v.cl == 1 && !v.lean) {
             int l2 = 0;
             AS_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, s->device));
             if (2.0 * s->sm_count * (double)vals * v.bytes_per_value > 0.75 * l2) gs_bt = 1024;
@@ -925,12 +942,12 @@ int build_groups(as_solver* s) {
         // shared memory: a trajectory that leaves no room for a second CTA on the SM gets
         // the largest CTA (more warps to hide the clause phase's latencies)
         int sm_bt = bt;
-        if (!v.gs) {
+        if (!v.gs || v.lean) {
             const int r = shared_cta_threads(sbytes, bt, s->device, &sm_bt);
             if (r) return r;
         }
-        G.bt = s->forced_bt ? s->forced_bt : (v.gs ? (v.cl > 1 ? 1024 : gs_bt) : sm_bt);
-        G.smem = v.gs ? 0 : sbytes;
+        G.bt = s->forced_bt ? s->forced_bt : (v.gs && !v.lean ? (v.cl > 1 ? 1024 : gs_bt) : sm_bt);
+        G.smem = sbytes;
         AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem));
         int occ = 0;
         if (v.cl > 1) {

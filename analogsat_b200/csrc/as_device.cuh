@@ -40,11 +40,11 @@ struct DevInstance {
     int tanh;
     double q, b;
     // Lean FP32 solver layout (solve_kernel_fast), or null when the instance does not
-    // qualify: clause-major literal words flit[m * k + q] that carry shared-memory byte
-    // offsets -- bit 31 negated literal, bits 14-29 the byte offset of the literal's
-    // contribution slot, bits 0-13 the byte offset of its spin (the spins sit at offset 0
-    // of the dynamic shared memory, the slots at cs_off, the interleaved RK stage rows
-    // at rows_off).
+    // qualify: clause-major literal words flit[m * k + q] that carry shared-memory
+    // addressing -- bit 31 negated literal, bits 14-30 the literal's contribution slot,
+    // bits 0-13 the byte offset of its spin (the spins sit at offset 0 of the dynamic
+    // shared memory, the slots at cs_off, the interleaved RK stage rows at rows_off or
+    // in a global slab).
     const uint32_t* flit;
     int cs_off, rows_off;
 };

@@ -8,11 +8,11 @@
 // down -- the shared-memory solver is issue bound, so its RHS rate is the inverse of
 // the instructions it executes per clause and stage:
 //
-//  * Literal words carry shared-memory byte offsets (DevInstance::flit): bits 0-13 the
+//  * Literal words carry shared-memory addressing (DevInstance::flit): bits 0-13 the
 //    byte offset of the literal's spin (the spins start at offset 0 of the dynamic
-//    shared memory), bits 14-29 the byte offset of its contribution slot, bit 31 the
-//    sign.  A spin gather is one mask and one load, a contribution store a shift, a
-//    mask and a store: no base-pointer arithmetic.
+//    shared memory), bits 14-30 the index of its contribution slot, bit 31 the sign.
+//    A spin gather is one mask and one load, a contribution store a shift, a mask, a
+//    scaled add and a store.
 //  * Literal words are clause-major (flit[m * K + q]), so a clause's K words are
 //    loads at immediate offsets from one pointer that advances once per clause.
 //  * The six RK vectors of an element are interleaved, [e][X, K1, K2, K3, K4, K5]
@@ -23,6 +23,12 @@
 //    own thread, no barrier).
 //  * No model branches: instances with the tanh variant or a bias term use
 //    solve_kernel.
+//  * ROWS_G: the interleaved RK rows live in a per-CTA slab of global memory
+//    (L2-resident while the slabs in flight fit) and only the spins and the
+//    contribution slots in shared memory -- the gathers and scatters stay on chip,
+//    the rows stream at 24 bytes per element.  This takes instances up to N < 4096
+//    whose spins and slots fit one SM (N=1000..4000 at alpha 4.25), where the
+//    all-shared layout stops at N of about 1,240.
 // The bank-aware clause grouping of the FP32 packing applies unchanged: a literal's
 // spin and its slot both sit in bank (internal variable mod 32).
 #pragma once
@@ -33,12 +39,13 @@
 
 namespace asb {
 
-// Shared-memory byte offsets of the lean layout for an instance, and whether it
-// qualifies (spin offsets below 16 KB, slot offsets below 64 KB).
+// Shared-memory byte offsets of the lean layout for an instance, and whether its
+// literal words can carry them (spin offsets below 16 KB, slot indices below 2^17).
+// bytes: shared memory with the rows on chip; bytes_g: without them (ROWS_G).
 struct FastLayout {
     bool ok = false;
     int cs_off = 0, rows_off = 0;
-    size_t bytes = 0;
+    size_t bytes = 0, bytes_g = 0;
 };
 __host__ __device__ inline FastLayout fast_layout(int n, int m, int nslots) {
     FastLayout L;
@@ -46,7 +53,8 @@ __host__ __device__ inline FastLayout fast_layout(int n, int m, int nslots) {
     const long long cs_end = (long long)L.cs_off + 4ll * (nslots + 1);
     L.rows_off = (int)((cs_end + 15) / 16 * 16);
     L.bytes = (size_t)L.rows_off + 24ull * (size_t)(n + m);
-    L.ok = 4ll * n < 16384 && (long long)L.cs_off + 4ll * nslots < 65536;
+    L.bytes_g = (size_t)L.rows_off;
+    L.ok = 4ll * n < 16384 && nslots < (1 << 17);
     return L;
 }
 
@@ -77,22 +85,44 @@ __device__ __forceinline__ void sts(uint32_t a, float v) {
 struct Row6 {
     float x = 0.f, k1 = 0.f, k2 = 0.f, k3 = 0.f, k4 = 0.f, k5 = 0.f;
 };
-template <int S>
-__device__ __forceinline__ Row6 load_row(uint32_t r) {
+// Where the interleaved rows live: shared memory (32-bit shared-window addresses) or a
+// per-CTA global slab.  at(e) is element e's row; ld/ld2/st take the float index in it.
+template <bool G> struct RowStore;
+template <> struct RowStore<false> {
+    using Ref = uint32_t;
+    uint32_t base;
+    __device__ __forceinline__ Ref at(int e) const { return base + 24u * (uint32_t)e; }
+    __device__ __forceinline__ static Ref advance(Ref r, int elems) { return r + 24u * (uint32_t)elems; }
+    __device__ __forceinline__ static float ld(Ref r, int i) { return lds(r + 4u * i); }
+    __device__ __forceinline__ static float2 ld2(Ref r, int i) { return lds2(r + 4u * i); }
+    __device__ __forceinline__ static void st(Ref r, int i, float v) { sts(r + 4u * i, v); }
+};
+template <> struct RowStore<true> {
+    using Ref = float*;
+    float* base;
+    __device__ __forceinline__ Ref at(int e) const { return base + 6ll * e; }
+    __device__ __forceinline__ static Ref advance(Ref r, int elems) { return r + 6ll * elems; }
+    __device__ __forceinline__ static float ld(Ref r, int i) { return r[i]; }
+    __device__ __forceinline__ static float2 ld2(Ref r, int i) { return *reinterpret_cast<const float2*>(r + i); }
+    __device__ __forceinline__ static void st(Ref r, int i, float v) { r[i] = v; }
+};
+
+template <int S, typename R>
+__device__ __forceinline__ Row6 load_row(typename R::Ref r) {
     Row6 o;
     if constexpr (S == 1) {
-        o.x = lds(r);
+        o.x = R::ld(r, 0);
     } else {
-        const float2 a = lds2(r);
+        const float2 a = R::ld2(r, 0);
         o.x = a.x; o.k1 = a.y;
-        if constexpr (S == 3) o.k2 = lds(r + 8);
+        if constexpr (S == 3) o.k2 = R::ld(r, 2);
         if constexpr (S >= 4) {
-            const float2 b = lds2(r + 8);
+            const float2 b = R::ld2(r, 2);
             o.k2 = b.x; o.k3 = b.y;
         }
-        if constexpr (S == 5) o.k4 = lds(r + 16);
+        if constexpr (S == 5) o.k4 = R::ld(r, 4);
         if constexpr (S == 6) {
-            const float2 c = lds2(r + 16);
+            const float2 c = R::ld2(r, 4);
             o.k4 = c.x; o.k5 = c.y;
         }
     }
@@ -113,7 +143,7 @@ __device__ __forceinline__ float lit_factor(uint32_t sm0, uint32_t w) {
 // K_m, the leave-one-out products in CpuProdWrapper order, contributions into their
 // slots; returns du_m = K_m^2 / ln 2.  Same operations as clause_phase<float, true, K>.
 template <int K>
-__device__ __forceinline__ float fast_clause(uint32_t sm0, const uint32_t* lp, float am, float knorm) {
+__device__ __forceinline__ float fast_clause(uint32_t sm0, uint32_t cs0, const uint32_t* lp, float am, float knorm) {
     uint32_t w[K];
     float f[K];
 #pragma unroll
@@ -137,13 +167,14 @@ __device__ __forceinline__ float fast_clause(uint32_t sm0, const uint32_t* lp, f
             }
         }
         const float rr = (r + r) * prod;  // (2r) prod == 2 (r prod) above the subnormals
-        sts(sm0 + ((w[q] >> 14) & 0xFFFFu), __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u)));
+        sts(cs0 + 4u * ((w[q] >> 14) & 0x1FFFFu), __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u)));
     }
     return km * km * kInvLn2;
 }
 
-template <int K>
+template <int K, bool ROWS_G>
 __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
+    using R = RowStore<ROWS_G>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red_d[36];
     __shared__ int red_i[33];
@@ -171,15 +202,16 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         const int n = I.n, m = I.m;
         float* const sy = reinterpret_cast<float*>(smem_raw);
         float* const cs = reinterpret_cast<float*>(smem_raw + I.cs_off);
-        float* const rows = reinterpret_cast<float*>(smem_raw + I.rows_off);
-        const uint32_t rows0 = sm0 + (uint32_t)I.rows_off;  // row e at rows0 + 24 e
+        R rs;
+        if constexpr (ROWS_G) rs.base = reinterpret_cast<float*>(P.slab) + (long long)blockIdx.x * P.slab_stride;
+        else rs.base = sm0 + (uint32_t)I.rows_off;
         const uint32_t cs0 = sm0 + (uint32_t)I.cs_off;
         float* G = reinterpret_cast<float*>(P.states) + P.unit_state[u];
         const float knorm = (float)ldexp(1.0, -I.k);
 
         // initial state: public spins to internal order, a -> log2 a
-        for (int i = tid; i < n; i += nt) rows[6 * __ldg(I.iperm + i)] = G[i];
-        for (int j = tid; j < m; j += nt) rows[6 * (n + __ldg(I.icperm + j))] = log2f(G[n + j]);
+        for (int i = tid; i < n; i += nt) R::st(rs.at(__ldg(I.iperm + i)), 0, G[i]);
+        for (int j = tid; j < m; j += nt) R::st(rs.at(n + __ldg(I.icperm + j)), 0, log2f(G[n + j]));
         for (int j = tid; j <= I.nslots; j += nt) cs[j] = 0.0f;
         if (tid == 0) sy[n] = -1.0f;  // sentinel spin: padding literals are always FALSE
         g.sync();  // the scatter above wrote rows that other threads own in the stage loops
@@ -190,18 +222,18 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         auto eval = [&](auto stage, float hT, float h0T, float& em) {
             constexpr int S = decltype(stage)::value;
             for (int v = tid; v < n; v += nt)
-                sts(sm0 + 4u * (uint32_t)v, row_input<S>(load_row<S>(rows0 + 24u * (uint32_t)v), hT));
+                sts(sm0 + 4u * (uint32_t)v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
             g.sync();
             const uint32_t* lp = I.flit + (size_t)tid * K;
-            uint32_t ra = rows0 + 24u * (uint32_t)(n + tid);
-            for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra += 24u * (uint32_t)nt) {
-                const Row6 o = load_row<S>(ra);
-                const float d = fast_clause<K>(sm0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+            typename R::Ref ra = rs.at(n + tid);
+            for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
+                const Row6 o = load_row<S, R>(ra);
+                const float d = fast_clause<K>(sm0, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
                 if constexpr (S < 6) {
-                    sts(ra + 4u * S, d);
+                    R::st(ra, S, d);
                 } else {
                     em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, d, hT, h0T, true));
-                    sts(ra + 8u, rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT));
+                    R::st(ra, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT));
                 }
             }
             g.sync();
@@ -212,13 +244,13 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 float sum = 0.0f;
 #pragma unroll 4
                 for (int k = r0; k < r1; k++, p += 128u) sum = sum + lds(p);
-                const uint32_t r = rows0 + 24u * (uint32_t)v;
+                const typename R::Ref r = rs.at(v);
                 if constexpr (S < 6) {
-                    sts(r + 4u * S, sum);
+                    R::st(r, S, sum);
                 } else {
-                    const Row6 o = load_row<6>(r);
+                    const Row6 o = load_row<6, R>(r);
                     em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
-                    sts(r + 8u, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
+                    R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
                 }
             }
         };
@@ -275,12 +307,12 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 // accept: the candidate state (slot 2) becomes the state, each element by
                 // the thread that owns it in the stage loops
                 for (int v = tid; v < n; v += nt) {
-                    const uint32_t r = rows0 + 24u * (uint32_t)v;
-                    sts(r, lds(r + 8u));
+                    const typename R::Ref r = rs.at(v);
+                    R::st(r, 0, R::ld(r, 2));
                 }
                 for (int c = tid; c < m; c += nt) {
-                    const uint32_t r = rows0 + 24u * (uint32_t)(n + c);
-                    sts(r, lds(r + 8u));
+                    const typename R::Ref r = rs.at(n + c);
+                    R::st(r, 0, R::ld(r, 2));
                 }
             }
             if (underflow) { status = SAT_UNDERFLOW; break; }
@@ -288,7 +320,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             if (interrupted) { status = SAT_ODE_INTERRUPTED; break; }
 
             // CpuSat::GetClauseViolationCount on the accepted state
-            for (int v = tid; v < n; v += nt) sts(sm0 + 4u * (uint32_t)v, lds(rows0 + 24u * (uint32_t)v));
+            for (int v = tid; v < n; v += nt) sts(sm0 + 4u * (uint32_t)v, R::ld(rs.at(v), 0));
             g.sync();
             int cnt = 0;
             {
@@ -336,8 +368,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
 
         // write back the final state in the public layout
         g.sync();
-        for (int i = tid; i < n; i += nt) G[i] = rows[6 * __ldg(I.iperm + i)];
-        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(rows[6 * (n + __ldg(I.icperm + j))]);
+        for (int i = tid; i < n; i += nt) G[i] = R::ld(rs.at(__ldg(I.iperm + i)), 0);
+        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(R::ld(rs.at(n + __ldg(I.icperm + j)), 0));
         if (tid == 0) {
             UnitResult r;
             r.time = t; r.hdid = hdid; r.status = status; r.steps = steps; r.attempts = attempts;

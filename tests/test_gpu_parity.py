@@ -387,3 +387,31 @@ def test_lean_kernel_matches_generic_kernel(golden, tag):
         assert np.array_equal(ra[key], rb[key]), key
     np.testing.assert_allclose(xb, xa, rtol=1e-6, atol=1e-6)
     print(tag, "bit-identical" if np.array_equal(xa, xb) else f"max diff {np.abs(xa - xb).max():.3g}")
+
+
+@pytest.mark.parametrize("n,m", [(1500, 6375), (3000, 12750)])
+def test_lean_kernel_global_rows_matches_generic_kernel(n, m):
+    """Instances beyond one SM's shared memory: the lean kernel with its interleaved RK
+    rows in a global slab (spins and contribution slots still in shared memory) against
+    the general kernel's global-storage mode -- same step, attempt and RHS counts, states
+    equal to FP32 rounding -- and the lean kernel is the one chosen by default."""
+    from analogsat_b200 import AS_PREC_F32_LOGA, SatProblem, SatSolver, _abi
+    from analogsat_b200.instances import make_instance, initial_states
+    lits, lens, _ = make_instance("planted", n, m, 3, seed=n)
+    p = SatProblem.from_arrays(lits, lens)
+    ics = initial_states(n, m, 6, seed=3, dtype=np.float32)
+    out, names = {}, {}
+    for kern in (_abi.AS_KERNEL_GENERIC, _abi.AS_KERNEL_AUTO):
+        s = SatSolver([p], precision=AS_PREC_F32_LOGA)
+        s.SetEpsilon(1e-6); s.SetBatchSize(25); s.SetMaxSteps(150); s.SetMaxTime(1e8)
+        s.SetKernel(kern)
+        s.SetSatStates(np.zeros(6, np.int32), ics)
+        s.Solve()
+        out[kern] = (s.results(), s.GetSatStates(np.float32).reshape(6, -1))
+        names[kern] = s.kernel_name()
+    assert names == {_abi.AS_KERNEL_GENERIC: "solve_kernel", _abi.AS_KERNEL_AUTO: "solve_kernel_fast"}
+    (ra, xa), (rb, xb) = out[_abi.AS_KERNEL_GENERIC], out[_abi.AS_KERNEL_AUTO]
+    for key in ("status", "steps", "attempts", "rhs", "violations"):
+        assert np.array_equal(ra[key], rb[key]), key
+    np.testing.assert_allclose(xb, xa, rtol=1e-6, atol=1e-6)
+    print(n, "bit-identical" if np.array_equal(xa, xb) else f"max diff {np.abs(xa - xb).max():.3g}")
