@@ -366,11 +366,6 @@ struct as_solver {
     DevBuf states, results, unit_inst, unit_state, unit_bits, queue, solved, deadline, best_bits, slab;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;  // orders a caller's stream with `stream`
-    // launch groups after the first run on side streams, forked from and joined back to
-    // the solve's stream, so a group's CTAs take the SMs that an earlier group's
-    // drained queue leaves idle
-    std::vector<cudaStream_t> side;
-    std::vector<cudaEvent_t> side_ev;  // [0] fork, [1 + g] join of group g
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
     bool groups_dirty = true;
@@ -381,8 +376,6 @@ struct as_solver {
         if (graph) cudaGraphExecDestroy(graph);
         if (ev_in) cudaEventDestroy(ev_in);
         if (ev_out) cudaEventDestroy(ev_out);
-        for (auto e : side_ev) cudaEventDestroy(e);
-        for (auto q : side) cudaStreamDestroy(q);
         if (stream) cudaStreamDestroy(stream);
     }
     void invalidate() { graph_valid = false; }
@@ -1041,23 +1034,9 @@ int record_solve(as_solver* s, cudaStream_t st) {
                                                (unsigned long long)(s->wall_budget * 1e9));
         AS_CUDA(cudaGetLastError());
     }
-    const size_t ng = s->groups.size();
-    while (s->side.size() + 1 < ng) {
-        cudaStream_t q = nullptr;
-        AS_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
-        s->side.push_back(q);
-    }
-    while (s->side_ev.size() < ng + 1) {
-        cudaEvent_t e = nullptr;
-        AS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        s->side_ev.push_back(e);
-    }
-    if (ng > 1) AS_CUDA(cudaEventRecord(s->side_ev[0], st));
-    for (size_t g = 0; g < ng; g++) {
+    for (size_t g = 0; g < s->groups.size(); g++) {
         const auto& G = s->groups[g];
         const Variant& v = vs[G.variant];
-        const cudaStream_t gst = g == 0 ? st : s->side[g - 1];
-        if (g > 0) AS_CUDA(cudaStreamWaitEvent(gst, s->side_ev[0], 0));
         const size_t smem = G.smem;
         const int occ = G.occ, ctas = G.ctas, units = G.u1 - G.u0;
         SolveParams P;
@@ -1090,18 +1069,16 @@ int record_solve(as_solver* s, cudaStream_t st) {
             cfg.gridDim = dim3(ctas);
             cfg.blockDim = dim3(G.bt);
             cfg.dynamicSmemBytes = smem;
-            cfg.stream = gst;
+            cfg.stream = st;
             cfg.attrs = &attr;
             cfg.numAttrs = 1;
             AS_CUDA(cudaLaunchKernelExC(&cfg, (const void*)v.fn, args));
         } else {
-            AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(G.bt), args, smem, gst));
+            AS_CUDA(cudaLaunchKernel((const void*)v.fn, dim3(ctas), dim3(G.bt), args, smem, st));
         }
-        if (g > 0) AS_CUDA(cudaEventRecord(s->side_ev[1 + g], gst));
         s->last_bt = G.bt; s->last_ctas = ctas; s->last_smem = (int)smem; s->last_occ = occ;
         s->last_kernel = v.name();
     }
-    for (size_t g = 1; g < ng; g++) AS_CUDA(cudaStreamWaitEvent(st, s->side_ev[1 + g], 0));
     return AS_OK;
 }
 
