@@ -405,6 +405,7 @@ def test_lean_kernel_global_rows_matches_generic_kernel(n, m):
         s = SatSolver([p], precision=AS_PREC_F32_LOGA)
         s.SetEpsilon(1e-6); s.SetBatchSize(25); s.SetMaxSteps(150); s.SetMaxTime(1e8)
         s.SetKernel(kern)
+        s.SetClusterSize(1)  # few trajectories would otherwise take a cluster of CTAs each
         s.SetSatStates(np.zeros(6, np.int32), ics)
         s.Solve()
         out[kern] = (s.results(), s.GetSatStates(np.float32).reshape(6, -1))
