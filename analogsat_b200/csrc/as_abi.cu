@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <ctime>
 #include <cmath>
@@ -67,6 +68,7 @@ struct DevBuf {
 struct DevicePool {
     int device = -1;
     DevBuf lit, litw, slotw, srow, perm, iperm, icperm, cperm, inst, flit;
+    DevBuf plit, pc0, psrow, pcnt, picperm;  // clause-parts layouts (lean global-rows form)
     std::vector<DevInstance> host_inst;
 
     template <typename V>
@@ -77,7 +79,8 @@ struct DevicePool {
         return AS_OK;
     }
 
-    int upload(const std::vector<const PackedProblem*>& pk, int dev) {
+    int upload(const std::vector<const PackedProblem*>& pk, int dev,
+               const std::vector<PartLayout>* parts = nullptr) {
         size_t nl = 0, nw = 0, nr = 0, np = 0, nc = 0;
         for (auto* q : pk) {
             nl += q->lit.size();
@@ -116,6 +119,34 @@ struct DevicePool {
         }
         AS_CUDA(flit.alloc(std::max<size_t>(fw.size(), 1) * 4));
         if (!fw.empty()) AS_CUDA(cudaMemcpy(flit.p, fw.data(), fw.size() * 4, cudaMemcpyHostToDevice));
+        // clause parts, concatenated over the problems that have them
+        std::vector<uint32_t> pw;
+        std::vector<int32_t> pc, ps, pi;
+        std::vector<uint16_t> pn;
+        std::vector<std::array<size_t, 5>> poff(pk.size(), std::array<size_t, 5>{0, 0, 0, 0, 0});
+        if (parts)
+            for (size_t i = 0; i < pk.size() && i < parts->size(); i++) {
+                const PartLayout& L = (*parts)[i];
+                if (L.nparts < 1) continue;
+                poff[i] = {pw.size(), pc.size(), ps.size(), pn.size(), pi.size()};
+                pw.insert(pw.end(), L.words.begin(), L.words.end());
+                pc.insert(pc.end(), L.c0.begin(), L.c0.end());
+                ps.insert(ps.end(), L.srow.begin(), L.srow.end());
+                pn.insert(pn.end(), L.cnt.begin(), L.cnt.end());
+                pi.insert(pi.end(), L.icperm.begin(), L.icperm.end());
+            }
+        AS_CUDA(plit.alloc(std::max<size_t>(pw.size(), 1) * 4));
+        AS_CUDA(pc0.alloc(std::max<size_t>(pc.size(), 1) * 4));
+        AS_CUDA(psrow.alloc(std::max<size_t>(ps.size(), 1) * 4));
+        AS_CUDA(pcnt.alloc(std::max<size_t>(pn.size(), 1) * 2));
+        AS_CUDA(picperm.alloc(std::max<size_t>(pi.size(), 1) * 4));
+        if (!pw.empty()) {
+            AS_CUDA(cudaMemcpy(plit.p, pw.data(), pw.size() * 4, cudaMemcpyHostToDevice));
+            AS_CUDA(cudaMemcpy(pc0.p, pc.data(), pc.size() * 4, cudaMemcpyHostToDevice));
+            AS_CUDA(cudaMemcpy(psrow.p, ps.data(), ps.size() * 4, cudaMemcpyHostToDevice));
+            AS_CUDA(cudaMemcpy(pcnt.p, pn.data(), pn.size() * 2, cudaMemcpyHostToDevice));
+            AS_CUDA(cudaMemcpy(picperm.p, pi.data(), pi.size() * 4, cudaMemcpyHostToDevice));
+        }
         host_inst.clear();
         size_t ol = 0, ow = 0, orr = 0, op = 0, oc = 0;
         for (auto* q : pk) {
@@ -139,6 +170,15 @@ struct DevicePool {
                 d.flit = fo >= 0 ? flit.as<uint32_t>() + fo : nullptr;
                 d.cs_off = L.cs_off;
                 d.rows_off = L.rows_off;
+                const size_t i = host_inst.size();
+                const PartLayout* PL = parts && i < parts->size() ? &(*parts)[i] : nullptr;
+                d.nparts = PL ? PL->nparts : 0;
+                d.part_slots = PL ? PL->max_slots : 0;
+                d.plit = d.nparts ? plit.as<uint32_t>() + poff[i][0] : nullptr;
+                d.part_c0 = d.nparts ? pc0.as<int32_t>() + poff[i][1] : nullptr;
+                d.part_srow = d.nparts ? psrow.as<int32_t>() + poff[i][2] : nullptr;
+                d.part_cnt = d.nparts ? pcnt.as<uint16_t>() + poff[i][3] : nullptr;
+                d.picperm = d.nparts ? picperm.as<int32_t>() + poff[i][4] : nullptr;
             }
             int r;
             if ((r = put(lit, ol, q->lit)) || (r = put(litw, ow, q->litw)) || (r = put(slotw, ow, q->slotw)) ||
@@ -213,7 +253,7 @@ const std::vector<Variant>& variants() {
 size_t solver_smem(const Variant& v, const PackedProblem& q) {
     if (v.lean) {
         const FastLayout L = fast_layout(q.n, q.m, q.nslots);
-        return v.gs ? L.bytes_g : L.bytes;
+        return v.gs ? (size_t)L.cs_off + 4 * (size_t)(q.lean_part_slots + 1) : L.bytes;
     }
     if (v.gs) return 0;
     return solve_smem_values(q.n, q.m, q.nslots) * v.bytes_per_value;
@@ -232,6 +272,7 @@ size_t solver_slab_values(const Variant& v, const PackedProblem& q) {
 bool fits(const Variant& v, const PackedProblem& q, int precision, size_t smem_limit) {
     const bool kok = v.exact ? q.k == v.kmax : q.k <= v.kmax;
     if (v.precision != precision || !kok) return false;
+    if (v.lean && v.gs) return standard_model(q) && q.lean_parts > 0 && solver_smem(v, q) <= smem_limit;
     if (v.lean) return standard_model(q) && q.compact && fast_layout(q.n, q.m, q.nslots).ok &&
                        solver_smem(v, q) <= smem_limit;
     if (v.gs) return true;
@@ -329,6 +370,7 @@ struct as_solver {
     int device = 0;
     int precision = AS_PREC_F32_LOGA;
     std::vector<PackedProblem> problems;
+    std::vector<PartLayout> parts;  // per problem: clause parts of the lean global-rows form
     DevicePool pool;
     int sm_count = 0;
     size_t smem_limit = 0;
@@ -741,14 +783,35 @@ int32_t as_solver_create(const as_problem* const* problems, int32_t num_problems
     if (r) return r;
     s->precision = precision;
     for (int i = 0; i < num_problems; i++) s->problems.push_back(const_cast<as_problem*>(problems[i])->packed(precision));
-    std::vector<const PackedProblem*> pk;
-    for (auto& q : s->problems) pk.push_back(&q);
-    r = s->pool.upload(pk, s->device);
-    if (r) return r;
     int optin = 0;
     AS_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
     AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, s->device));
     s->smem_limit = (size_t)optin - 1024;  // static shared memory of the kernel
+    // FP32 plain-CTDS instances beyond the all-shared lean layout: clause parts for the
+    // lean kernel's global-rows form, the fewest parts whose slots fit one SM
+    s->parts.assign(num_problems, PartLayout());
+    if (precision == AS_PREC_F32_LOGA)
+        for (int i = 0; i < num_problems; i++) {
+            auto& q = s->problems[i];
+            if (!standard_model(q) || (q.k != 3 && q.k != 4) || q.n >= 8191) continue;
+            const FastLayout L = fast_layout(q.n, q.m, q.nslots);
+            if (q.compact && L.ok && L.bytes <= s->smem_limit) continue;  // the all-shared form takes it
+            const HostProblem& hp = problems[i]->host;
+            for (int np = 1; np <= 4; np++) {
+                PartLayout PL;
+                if (!pack_parts(hp, q, np, PL)) break;
+                if ((size_t)L.cs_off + 4 * (size_t)(PL.max_slots + 1) <= s->smem_limit) {
+                    q.lean_parts = np;
+                    q.lean_part_slots = PL.max_slots;
+                    s->parts[i] = std::move(PL);
+                    break;
+                }
+            }
+        }
+    std::vector<const PackedProblem*> pk;
+    for (auto& q : s->problems) pk.push_back(&q);
+    r = s->pool.upload(pk, s->device, &s->parts);
+    if (r) return r;
     AS_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     for (auto& q : s->problems) {
         bool any = false;

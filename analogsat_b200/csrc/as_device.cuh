@@ -47,6 +47,17 @@ struct DevInstance {
     // in a global slab).
     const uint32_t* flit;
     int cs_off, rows_off;
+    // Clause parts of the lean kernel's global-rows form (PartLayout in as_problem.h):
+    // words plit[m * k + q] = sign | slot in the part's buffer << 13 | internal variable,
+    // part p's internal clauses [part_c0[p], part_c0[p + 1]), SELL rows part_srow[p *
+    // (nslices + 1) + g], occurrences part_cnt[p * n + v], its own clause order picperm
+    // (public -> internal); nparts = 0 when the instance has no such layout.
+    const uint32_t* plit;
+    const int32_t* part_c0;
+    const int32_t* part_srow;
+    const uint16_t* part_cnt;
+    const int32_t* picperm;
+    int nparts, part_slots;
 };
 
 constexpr float kInvLn2 = 1.4426950408889634f;  // d(log2 a)/dt = (da/dt) / (a ln 2)

@@ -172,6 +172,42 @@ __device__ __forceinline__ float fast_clause(uint32_t sm0, uint32_t cs0, const u
     return km * km * kInvLn2;
 }
 
+// The same on a clause-parts word (bits 0-12 internal variable, 13-29 slot, 31 sign).
+template <int K>
+__device__ __forceinline__ float part_clause(uint32_t sm0, uint32_t cs0, const uint32_t* lp, float am,
+                                             float knorm) {
+    uint32_t w[K];
+    float f[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) w[q] = ld_lit(lp + q);
+    float km = knorm;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        const float sv = lds(sm0 + 4u * (w[q] & 0x1FFFu));
+        f[q] = 1.0f - __int_as_float(__float_as_int(sv) ^ (int)(w[q] & 0x80000000u));
+        km = km * f[q];
+    }
+    const float r = (km * knorm) * am;
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+        float prod = 1.0f;
+        bool first = true;
+#pragma unroll
+        for (int l = 0; l < K; l++) {
+            if (l != q) {
+                prod = first ? f[l] : prod * f[l];
+                first = false;
+            }
+        }
+        const float rr = (r + r) * prod;
+        sts(cs0 + 4u * ((w[q] >> 13) & 0x1FFFFu), __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u)));
+    }
+    return km * km * kInvLn2;
+}
+
+// ROWS_G = false: rows, spins and slots in shared memory, words flit.  ROWS_G = true:
+// rows in the CTA's global slab, spins and slots in shared memory, clauses in parts
+// (words plit), each part's contributions summed before the next part reuses the slots.
 template <int K, bool ROWS_G>
 __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
     using R = RowStore<ROWS_G>;
@@ -210,9 +246,11 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         const float knorm = (float)ldexp(1.0, -I.k);
 
         // initial state: public spins to internal order, a -> log2 a
+        const int32_t* const icp = ROWS_G ? I.picperm : I.icperm;  // public -> internal clause
         for (int i = tid; i < n; i += nt) R::st(rs.at(__ldg(I.iperm + i)), 0, G[i]);
-        for (int j = tid; j < m; j += nt) R::st(rs.at(n + __ldg(I.icperm + j)), 0, log2f(G[n + j]));
-        for (int j = tid; j <= I.nslots; j += nt) cs[j] = 0.0f;
+        for (int j = tid; j < m; j += nt) R::st(rs.at(n + __ldg(icp + j)), 0, log2f(G[n + j]));
+        if constexpr (!ROWS_G)  // padding slots are read as zeros (the parts form reads counts)
+            for (int j = tid; j <= I.nslots; j += nt) cs[j] = 0.0f;
         if (tid == 0) sy[n] = -1.0f;  // sentinel spin: padding literals are always FALSE
         g.sync();  // the scatter above wrote rows that other threads own in the stage loops
 
@@ -224,6 +262,49 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             for (int v = tid; v < n; v += nt)
                 sts(sm0 + 4u * (uint32_t)v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
             g.sync();
+            if constexpr (ROWS_G) {
+                const int np = I.nparts, ns1 = ((n + 31) >> 5) + 1;
+                for (int pp = 0; pp < np; pp++) {
+                    const int c0 = ld_ro(I.part_c0 + pp), c1 = ld_ro(I.part_c0 + pp + 1);
+                    const uint32_t* lp = I.plit + (size_t)(c0 + tid) * K;
+                    typename R::Ref ra = rs.at(n + c0 + tid);
+                    for (int c = c0 + tid; c < c1; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
+                        const Row6 o = load_row<S, R>(ra);
+                        const float d = part_clause<K>(sm0, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+                        if constexpr (S < 6) {
+                            R::st(ra, S, d);
+                        } else {
+                            em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, d, hT, h0T, true));
+                            R::st(ra, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT));
+                        }
+                    }
+                    g.sync();
+                    // each variable's sum continues from the previous part (kept in slot S,
+                    // or for S = 6 in slot 2, whose K2 the stage-6 input has read already)
+                    constexpr int SLOT = S < 6 ? S : 2;
+                    const bool last = pp + 1 == np;
+                    for (int v = tid; v < n; v += nt) {
+                        const int cnt = (int)I.part_cnt[(size_t)pp * n + v];
+                        const int r0 = ld_ro(I.part_srow + (size_t)pp * ns1 + (v >> 5));
+                        uint32_t pa = cs0 + 4u * (uint32_t)(r0 * 32 + (v & 31));
+                        const typename R::Ref r = rs.at(v);
+                        float sum = pp == 0 ? 0.0f : R::ld(r, SLOT);
+#pragma unroll 4
+                        for (int k = 0; k < cnt; k++, pa += 128u) sum = sum + lds(pa);
+                        if (!last) {
+                            R::st(r, SLOT, sum);
+                        } else if constexpr (S < 6) {
+                            R::st(r, S, sum);
+                        } else {
+                            const Row6 o = load_row<6, R>(r);
+                            em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
+                            R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
+                        }
+                    }
+                    if (!last) g.sync();  // the next part's clauses reuse the slots
+                }
+                return;
+            }
             const uint32_t* lp = I.flit + (size_t)tid * K;
             typename R::Ref ra = rs.at(n + tid);
             for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
@@ -324,13 +405,14 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             g.sync();
             int cnt = 0;
             {
-                const uint32_t* lp = I.flit + (size_t)tid * K;
+                const uint32_t* lp = (ROWS_G ? I.plit : I.flit) + (size_t)tid * K;
                 for (int c = tid; c < m; c += nt, lp += (size_t)nt * K) {
                     bool sat = false;
 #pragma unroll
                     for (int q = 0; q < K; q++) {
                         const uint32_t w = ld_lit(lp + q);
-                        const bool tv = lds(sm0 + (w & 0x3FFFu)) > 0.0f;
+                        const uint32_t sa = ROWS_G ? 4u * (w & 0x1FFFu) : (w & 0x3FFFu);
+                        const bool tv = lds(sm0 + sa) > 0.0f;
                         sat |= (w & 0x80000000u) ? !tv : tv;
                     }
                     cnt += sat ? 0 : 1;
@@ -369,7 +451,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         // write back the final state in the public layout
         g.sync();
         for (int i = tid; i < n; i += nt) G[i] = R::ld(rs.at(__ldg(I.iperm + i)), 0);
-        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(R::ld(rs.at(n + __ldg(I.icperm + j)), 0));
+        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(R::ld(rs.at(n + __ldg(icp + j)), 0));
         if (tid == 0) {
             UnitResult r;
             r.time = t; r.hdid = hdid; r.status = status; r.steps = steps; r.attempts = attempts;

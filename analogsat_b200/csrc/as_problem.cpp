@@ -699,6 +699,102 @@ void schedule_balanced(const HostProblem& p, PackedProblem& q, bool pairs,
 
 }  // namespace
 
+bool pack_parts(const HostProblem& p, const PackedProblem& q, int nparts, PartLayout& out) {
+    out = PartLayout();
+    if (p.n >= 8191 || p.k > 16 || nparts < 1 || (int)q.iperm.size() != p.n) return false;
+    const int n = p.n, m = p.m, k = p.k, ns = (n + 31) / 32;
+    if (nparts == 1) {
+        // one part is the FP32 packing itself: its clause grouping, literal order and slots
+        if (q.nslots >= (1 << 17)) return false;
+        out.nparts = 1;
+        out.max_slots = q.nslots;
+        out.c0 = {0, m};
+        out.srow = q.srow;
+        out.cperm = q.cperm;
+        out.icperm = q.icperm;
+        out.cnt.assign(n, 0);
+        out.words.assign((size_t)m * k, 0);
+        for (int mi = 0; mi < m; mi++)
+            for (int qq = 0; qq < k; qq++) {
+                const size_t idx = (size_t)qq * q.mp + mi;
+                const uint32_t v = q.litw[idx] & 0x7fffffffu;
+                if ((int)v < n) out.cnt[v]++;
+                out.words[(size_t)mi * k + qq] = (q.litw[idx] & 0x80000000u) | (q.slotw[idx] << 13) | v;
+            }
+        return true;
+    }
+    out.nparts = nparts;
+    out.c0.assign(nparts + 1, 0);
+    out.srow.assign((size_t)nparts * (ns + 1), 0);
+    out.cnt.assign((size_t)nparts * n, 0);
+    out.cperm.resize(m);
+    out.icperm.resize(m);
+    out.words.assign((size_t)m * k, 0);
+    std::vector<int32_t> slot_of(p.storage.size(), 0);
+    int mi0 = 0;
+    for (int pp = 0; pp < nparts; pp++) {
+        const int j0 = (int)((long long)m * pp / nparts), j1 = (int)((long long)m * (pp + 1) / nparts);
+        out.c0[pp] = mi0;
+        // occurrences per internal variable in this part, SELL rows per slice
+        uint16_t* cnt = out.cnt.data() + (size_t)pp * n;
+        for (int j = j0; j < j1; j++)
+            for (int i = 0; i < p.length[j]; i++) {
+                const int v = q.iperm[std::abs(p.storage[p.start[j] + i]) - 1];
+                if (cnt[v] == 0xFFFF) return false;
+                cnt[v]++;
+            }
+        int32_t* srow = out.srow.data() + (size_t)pp * (ns + 1);
+        for (int g = 0; g < ns; g++) {
+            int w = 0;
+            for (int l = 0; l < 32 && g * 32 + l < n; l++) w = std::max(w, (int)cnt[g * 32 + l]);
+            srow[g + 1] = srow[g] + w;
+        }
+        const int nslots = srow[ns] * 32;
+        if (nslots >= (1 << 17)) { out = PartLayout(); return false; }
+        out.max_slots = std::max(out.max_slots, nslots);
+        std::vector<int32_t> rank(n, 0);
+        for (int j = j0; j < j1; j++)
+            for (int i = 0; i < p.length[j]; i++) {
+                const int v = q.iperm[std::abs(p.storage[p.start[j] + i]) - 1];
+                slot_of[p.start[j] + i] = (srow[v >> 5] + rank[v]++) * 32 + (v & 31);
+            }
+        // bank-aware warp grouping of this part's clauses (banks: internal variable mod 32)
+        HostProblem sub;
+        sub.n = n;
+        sub.k = k;
+        for (int j = j0; j < j1; j++) {
+            sub.start.push_back((int32_t)sub.storage.size());
+            sub.length.push_back(p.length[j]);
+            for (int i = 0; i < p.length[j]; i++) sub.storage.push_back(p.storage[p.start[j] + i]);
+        }
+        sub.m = j1 - j0;
+        PackedProblem tq;
+        tq.iperm = q.iperm;
+        std::vector<std::vector<int8_t>> order;
+        if (sub.m > 0) schedule_balanced(sub, tq, false, order);
+        for (int t = 0; t < sub.m; t++) {
+            const int j = j0 + tq.cperm[t], mi = mi0 + t;
+            out.cperm[mi] = j;
+            out.icperm[j] = mi;
+            for (int qq = 0; qq < k; qq++) {
+                const int li = qq < (int)order[t].size() ? order[t][qq] : -1;
+                uint32_t w;
+                if (li < 0) {
+                    w = ((uint32_t)nslots << 13) | (uint32_t)n;  // sentinel: spin -1, trash slot
+                } else {
+                    const int lit = p.storage[p.start[j] + li];
+                    const uint32_t v = (uint32_t)q.iperm[std::abs(lit) - 1];
+                    w = (lit < 0 ? 0x80000000u : 0u) | ((uint32_t)slot_of[p.start[j] + li] << 13) | v;
+                }
+                out.words[(size_t)mi * k + qq] = w;
+            }
+        }
+        mi0 += sub.m;
+    }
+    out.c0[nparts] = mi0;
+    return true;
+}
+
 PackedProblem pack(const HostProblem& p, int mode) {
     const bool permute_literals = mode != kPackReference;
     PackedProblem q;

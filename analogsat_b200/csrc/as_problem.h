@@ -99,7 +99,32 @@ struct PackedProblem {
     // CpuSatTanh with slope q, b the bias coefficient (ISat::Set_B; 0 = off).
     int tanh = 0;
     double q = 1.1, b = 0.0;
+    // clause parts of the lean FP32 kernel's global-rows form (0: none) and the slots of
+    // the largest part (set by the solver that builds the PartLayout)
+    int lean_parts = 0, lean_part_slots = 0;
 };
+
+// Clause parts of the lean FP32 solver's global-rows form: the clauses are split by
+// public index into `nparts` ranges, each with its own bank-aware warp grouping and
+// its own SELL contribution slots (rows of a variable in public clause order), all
+// parts sharing one shared-memory slot buffer of max_slots + 1 entries.  The variable
+// phase of part p continues each variable's sum from part p - 1, so the sums run in
+// the reference's order.  Words are clause-major, internal clause order (parts
+// concatenated): bit 31 negated literal, bits 13-29 the slot in its part's buffer,
+// bits 0-12 the internal variable (N < 8191; sentinel N, slot = the part's trash slot).
+struct PartLayout {
+    int nparts = 0;
+    int max_slots = 0;               // largest part's slot count (its trash slot excluded)
+    std::vector<int32_t> c0;         // [nparts + 1] first internal clause of each part
+    std::vector<int32_t> srow;       // [nparts][nslices + 1] SELL row offsets per part
+    std::vector<uint16_t> cnt;       // [nparts][n] occurrences of internal variable v in part p
+    std::vector<int32_t> cperm;      // internal -> public clause
+    std::vector<int32_t> icperm;     // public -> internal clause
+    std::vector<uint32_t> words;     // [m][k]
+};
+// Builds the parts layout of an instance on the variable order of its FP32 packing q;
+// false (layout empty) when N >= 8191 or a part has 2^17 slots or more.
+bool pack_parts(const HostProblem& p, const PackedProblem& q, int nparts, PartLayout& out);
 
 enum PackMode : int {
     kPackReference = 0,  // reference literal order (FP64, bit-identical products)

@@ -2,7 +2,8 @@
 // instances, all three packing modes: every internal clause carries exactly its public
 // literals (sign and variable), every literal owns one distinct contribution slot in
 // its variable's SELL row, rows follow the public (clause, literal) order, the
-// permutations are inverse pairs, and the bank-group diagnostics are at least ideal.
+// permutations are inverse pairs, and the bank-group diagnostics are at least ideal;
+// and the clause-parts layout of the lean kernel's global-rows form.
 // Built with g++ against the host sources only (no CUDA).  Exit code 0 = all good.
 #include "../../analogsat_b200/csrc/as_problem.h"
 
@@ -75,6 +76,65 @@ static int check(const HostProblem& hp, int mode) {
     return 0;
 }
 
+// Clause parts (pack_parts): every public clause once, parts as public-index ranges,
+// each literal one distinct slot of its part's buffer in its variable's SELL column,
+// rows in public clause order within the part, occurrence counts consistent.
+static int check_parts(const HostProblem& hp, int nparts) {
+    const PackedProblem q = pack(hp, kPackF32);
+    PartLayout L;
+    if (!pack_parts(hp, q, nparts, L)) return hp.n >= 8191 ? 0 : 30;
+    const int n = q.n, m = q.m, k = q.k, ns = (n + 31) / 32;
+    if (L.nparts != nparts || (int)L.c0.size() != nparts + 1 || L.c0[nparts] != m) return 31;
+    for (int c = 0; c < m; c++)
+        if (L.icperm[L.cperm[c]] != c) return 32;
+    for (int pp = 0; pp < nparts; pp++) {
+        const int j0 = (int)((long long)m * pp / nparts), j1 = (int)((long long)m * (pp + 1) / nparts);
+        const int32_t* srow = L.srow.data() + (size_t)pp * (ns + 1);
+        const int nslots = srow[ns] * 32;
+        if (nslots > L.max_slots) return 33;
+        std::vector<int> owner(nslots + 1, -1);
+        std::vector<std::vector<std::pair<int, int>>> rows(n);
+        std::vector<int> cnt(n, 0);
+        for (int mi = L.c0[pp]; mi < L.c0[pp + 1]; mi++) {
+            const int j = L.cperm[mi];
+            if (j < j0 || j >= j1) return 34;
+            std::vector<long> want, got;
+            for (int i = 0; i < hp.length[j]; i++) {
+                const int lit = hp.storage[hp.start[j] + i];
+                want.push_back(2L * q.iperm[std::abs(lit) - 1] + (lit < 0));
+            }
+            for (int s = 0; s < k; s++) {
+                const uint32_t w = L.words[(size_t)mi * k + s];
+                const int v = (int)(w & 0x1FFFu), slot = (int)((w >> 13) & 0x1FFFFu);
+                if (v == n) {
+                    if (slot != nslots || (w >> 31)) return 35;
+                    continue;
+                }
+                if (v > n || slot >= nslots || owner[slot] >= 0 || (slot & 31) != (v & 31)) return 36;
+                owner[slot] = mi;
+                const int row = slot >> 5;
+                if (row < srow[v >> 5] || row >= srow[(v >> 5) + 1]) return 37;
+                rows[v].push_back({row, j});
+                cnt[v]++;
+                got.push_back(2L * v + (w >> 31));
+            }
+            std::sort(want.begin(), want.end());
+            std::sort(got.begin(), got.end());
+            if (want != got) return 38;
+        }
+        for (int v = 0; v < n; v++) {
+            if (cnt[v] != (int)L.cnt[(size_t)pp * n + v]) return 39;
+            auto r = rows[v];
+            std::sort(r.begin(), r.end());
+            for (size_t t = 0; t < r.size(); t++) {
+                if (r[t].first != srow[v >> 5] + (int)t) return 40;
+                if (t && r[t].second < r[t - 1].second) return 41;
+            }
+        }
+    }
+    return 0;
+}
+
 int main() {
     int cases = 0;
     for (int trial = 0; trial < 40; trial++) {
@@ -101,6 +161,14 @@ int main() {
             cases++;
             if (r) {
                 std::printf("FAIL trial %d mode %d n %d m %d k %d: code %d\n", trial, mode, n, m, k, r);
+                return r;
+            }
+        }
+        for (int np : {1, 2, 3}) {
+            const int r = check_parts(hp, np);
+            cases++;
+            if (r) {
+                std::printf("FAIL trial %d parts %d n %d m %d k %d: code %d\n", trial, np, n, m, k, r);
                 return r;
             }
         }

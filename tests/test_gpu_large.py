@@ -151,3 +151,31 @@ def test_maxsat_scale_instance_runs(oracle):
         assert r["violations"][i] == oracle.violations(op, fin[i].astype(np.float64))
         best = s.GetBestAssignment(i)
         assert oracle.violations(op, np.where(best, 1.0, -1.0)) == r["min_violations"][i]
+
+
+def test_lean_kernel_in_two_clause_parts_vs_fp64(oracle):
+    """N=4800, M=20400: the contribution slots of the whole instance (240 KB) do not fit
+    one SM, so the lean kernel's global-rows form splits every RHS into two clause parts
+    that reuse one slot buffer, the sums continuing from part to part.  FP32 against the
+    FP64 solution of the same ODE at the same analog time (oracle at eps 1e-10): 1e-5
+    relative to max(|x|, 1), as for the other FP32 paths."""
+    from analogsat_b200 import SatProblem
+    from analogsat_b200.instances import make_instance, initial_states
+    n, m = 4800, 20400
+    lits, lens, _ = make_instance("planted", n, m, 3, seed=48)
+    p = SatProblem.from_arrays(lits, lens)
+    ics = initial_states(n, m, 3, seed=5, dtype=np.float32)
+    s = _solver([p], 0, eps=1e-6, batch=20, maxsteps=20)
+    s.SetClusterSize(1)
+    s.SetSatStates(np.zeros(3, np.int32), ics)
+    s.Solve()
+    assert s.kernel_name() == "solve_kernel_fast"
+    assert s.launch_shape()["smem_bytes"] < 160 * 1024  # one part's slots, not the whole 240 KB
+    r = s.results()
+    X = s.GetSatStates(np.float32).reshape(3, n + m)
+    op = oracle.problem(lits, lens)
+    for t in range(3):
+        assert r["steps"][t] == 20
+        o = oracle.integrate_to(op, ics[t].astype(np.float64), r["time"][t], eps=1e-10)
+        err = np.abs(X[t] - o["state"]) / np.maximum(np.abs(o["state"]), 1.0)
+        assert err.max() <= 1e-5, err.max()
