@@ -154,7 +154,7 @@ def test_maxsat_scale_instance_runs(oracle):
 
 
 def test_lean_kernel_in_two_clause_parts_vs_fp64(oracle):
-    """N=4800, M=20400: the contribution slots of the whole instance (240 KB) do not fit
+    """N=4800, M=20400: the contribution slots of the whole instance (about 245 KB) do not fit
     one SM, so the lean kernel's global-rows form splits every RHS into two clause parts
     that reuse one slot buffer, the sums continuing from part to part.  FP32 against the
     FP64 solution of the same ODE at the same analog time (oracle at eps 1e-10): 1e-5
@@ -170,7 +170,8 @@ def test_lean_kernel_in_two_clause_parts_vs_fp64(oracle):
     s.SetSatStates(np.zeros(3, np.int32), ics)
     s.Solve()
     assert s.kernel_name() == "solve_kernel_fast"
-    assert s.launch_shape()["smem_bytes"] < 160 * 1024  # one part's slots, not the whole 240 KB
+    # the whole instance's slots exceed one SM; the launch holds one part's
+    assert 4 * p.layout_stats()["nslots"] > 227 * 1024 >= s.launch_shape()["smem_bytes"]
     r = s.results()
     X = s.GetSatStates(np.float32).reshape(3, n + m)
     op = oracle.problem(lits, lens)
