@@ -74,11 +74,48 @@ constexpr double b21 = 0.2, b31 = 3.0 / 40.0, b32 = 9.0 / 40.0, b41 = 0.3, b42 =
                  dc4 = c4 - 13525.0 / 55296.0, dc6 = c6 - 0.25;
 }  // namespace ck
 
-// Stage input y_S = x + h * sum_j b_Sj k_j in the reference's expression order.
+// FP32: y = x + h (sum_j b_j k_j), the sum formed left to right with fused
+// multiply-adds in a fixed pattern (u = b_1 k_1; u = fma(b_j, k_j, u); y = fma(h, u, x)):
+// explicit, so every kernel rounds the same way whatever the compiler would otherwise
+// contract.  B holds the coefficients in order.
+template <int NK>
+__device__ __forceinline__ float fma_sum(const float (&b)[NK], const float (&k)[NK]) {
+    float u = __fmul_rn(b[0], k[0]);
+#pragma unroll
+    for (int j = 1; j < NK; j++) u = __fmaf_rn(b[j], k[j], u);
+    return u;
+}
+template <int NK>
+__device__ __forceinline__ float fma_chain(const float (&b)[NK], const float (&k)[NK], float h, float x) {
+    return __fmaf_rn(h, fma_sum<NK>(b, k), x);
+}
+
+// Stage input y_S = x + h * sum_j b_Sj k_j in the reference's expression order
+// (FP64: every operation rounded as the reference rounds it; FP32: fma_chain).
 template <int S, typename T>
 __device__ __forceinline__ T stage_in(T x, T k1, T k2, T k3, T k4, T k5, T h) {
     using A = Arith<T>;
     if constexpr (S == 1) return x;
+    if constexpr (sizeof(T) == 4) {
+        if constexpr (S == 2) return __fmaf_rn(__fmul_rn((float)ck::b21, h), k1, x);
+        if constexpr (S == 3) {
+            const float b[2] = {(float)ck::b31, (float)ck::b32}, k[2] = {k1, k2};
+            return fma_chain<2>(b, k, h, x);
+        }
+        if constexpr (S == 4) {
+            const float b[3] = {(float)ck::b41, (float)ck::b42, (float)ck::b43}, k[3] = {k1, k2, k3};
+            return fma_chain<3>(b, k, h, x);
+        }
+        if constexpr (S == 5) {
+            const float b[4] = {(float)ck::b51, (float)ck::b52, (float)ck::b53, (float)ck::b54}, k[4] = {k1, k2, k3, k4};
+            return fma_chain<4>(b, k, h, x);
+        }
+        if constexpr (S == 6) {
+            const float b[5] = {(float)ck::b61, (float)ck::b62, (float)ck::b63, (float)ck::b64, (float)ck::b65},
+                        k[5] = {k1, k2, k3, k4, k5};
+            return fma_chain<5>(b, k, h, x);
+        }
+    }
     if constexpr (S == 2) return A::add(x, A::mul(A::mul(T(ck::b21), h), k1));
     if constexpr (S == 3) return A::add(x, A::mul(h, A::add(A::mul(T(ck::b31), k1), A::mul(T(ck::b32), k2))));
     if constexpr (S == 4)
@@ -101,9 +138,14 @@ __device__ __forceinline__ T stage_in(T x, T k1, T k2, T k3, T k4, T k5, T h) {
 template <typename T>
 __device__ __forceinline__ T rk_new(T x, T k1, T k3, T k4, T k6, T h) {
     using A = Arith<T>;
-    return A::add(x, A::mul(h, A::add(A::add(A::add(A::mul(T(ck::c1), k1), A::mul(T(ck::c3), k3)),
-                                             A::mul(T(ck::c4), k4)),
-                                      A::mul(T(ck::c6), k6))));
+    if constexpr (sizeof(T) == 4) {
+        const float b[4] = {(float)ck::c1, (float)ck::c3, (float)ck::c4, (float)ck::c6}, k[4] = {k1, k3, k4, k6};
+        return fma_chain<4>(b, k, h, x);
+    } else {
+        return A::add(x, A::mul(h, A::add(A::add(A::add(A::mul(T(ck::c1), k1), A::mul(T(ck::c3), k3)),
+                                                 A::mul(T(ck::c4), k4)),
+                                          A::mul(T(ck::c6), k6))));
+    }
 }
 
 // Error ratio |xerr / xscal| of one element (CpuRungeKutta.cpp:214, 233-235) with
@@ -126,9 +168,10 @@ __device__ __forceinline__ double rk_err_ratio(double x, double k1, double k3, d
 }
 __device__ __forceinline__ float rk_err_ratio(float x, float k1, float k3, float k4, float k5,
                                               float k6, float h, float h0, bool logw) {
-    const float e = h * (float(ck::dc1) * k1 + float(ck::dc3) * k3 + float(ck::dc4) * k4 +
-                         float(ck::dc5) * k5 + float(ck::dc6) * k6);
-    const float sc = (logw ? kInvLn2 : fabsf(x)) + fabsf(k1 * h0) + 1e-20f;
+    const float b[5] = {(float)ck::dc1, (float)ck::dc3, (float)ck::dc4, (float)ck::dc5, (float)ck::dc6},
+                k[5] = {k1, k3, k4, k5, k6};
+    const float e = __fmul_rn(h, fma_sum<5>(b, k));
+    const float sc = __fadd_rn(__fadd_rn(logw ? kInvLn2 : fabsf(x), fabsf(__fmul_rn(k1, h0))), 1e-20f);
     return __fdividef(fabsf(e), sc);
 }
 
