@@ -262,7 +262,8 @@ size_t solver_smem(const Variant& v, const PackedProblem& q) {
 // Values of a trajectory's per-CTA global slab (global-storage variants).
 size_t solver_slab_values(const Variant& v, const PackedProblem& q) {
     if (!v.gs) return 0;
-    if (v.lean) return 6 * (size_t)(q.n + q.m);  // the interleaved RK rows
+    if (v.lean)  // the RK rows, blocked by 32 elements, clauses from the next block
+        return 6 * (size_t)(row_clause_base<true>(q.n) + ((q.m + 31) & ~31));
     return solve_smem_values(q.n, q.m, q.nslots);
 }
 

@@ -23,12 +23,13 @@
 //    own thread, no barrier).
 //  * No model branches: instances with the tanh variant or a bias term use
 //    solve_kernel.
-//  * ROWS_G: the interleaved RK rows live in a per-CTA slab of global memory
-//    (L2-resident while the slabs in flight fit) and only the spins and the
-//    contribution slots in shared memory -- the gathers and scatters stay on chip,
-//    the rows stream at 24 bytes per element.  This takes instances up to N < 4096
-//    whose spins and slots fit one SM (N=1000..4000 at alpha 4.25), where the
-//    all-shared layout stops at N of about 1,240.
+//  * ROWS_G: the RK rows live in a per-CTA slab of global memory (L2-resident while
+//    the slabs in flight fit), blocked by 32 elements so that every row access of a
+//    warp is one coalesced line per field, and only the spins and the contribution
+//    slots in shared memory -- the gathers and scatters stay on chip.  With the
+//    clauses in parts (each part's contributions summed before the next part reuses
+//    the slots) this takes instances up to N < 8191, where the all-shared layout
+//    stops at N of about 1,240.
 // The bank-aware clause grouping of the FP32 packing applies unchanged: a literal's
 // spin and its slot both sit in bank (internal variable mod 32).
 #pragma once
@@ -97,15 +98,23 @@ template <> struct RowStore<false> {
     __device__ __forceinline__ static float2 ld2(Ref r, int i) { return lds2(r + 4u * i); }
     __device__ __forceinline__ static void st(Ref r, int i, float v) { sts(r + 4u * i, v); }
 };
+// In global memory the rows are blocked by 32 elements, [e / 32][X, K1..K5][e % 32]: a
+// warp's 32 consecutive elements read or write one field as one 128-byte line (an
+// interleaved 24-byte row would spread a warp's 32-bit store over 24 sectors).
+// advance() takes a multiple of 32 elements.
 template <> struct RowStore<true> {
     using Ref = float*;
     float* base;
-    __device__ __forceinline__ Ref at(int e) const { return base + 6ll * e; }
+    __device__ __forceinline__ Ref at(int e) const { return base + 192ll * (e >> 5) + (e & 31); }
     __device__ __forceinline__ static Ref advance(Ref r, int elems) { return r + 6ll * elems; }
-    __device__ __forceinline__ static float ld(Ref r, int i) { return r[i]; }
-    __device__ __forceinline__ static float2 ld2(Ref r, int i) { return *reinterpret_cast<const float2*>(r + i); }
-    __device__ __forceinline__ static void st(Ref r, int i, float v) { r[i] = v; }
+    __device__ __forceinline__ static float ld(Ref r, int i) { return r[32 * i]; }
+    __device__ __forceinline__ static float2 ld2(Ref r, int i) { return make_float2(r[32 * i], r[32 * i + 32]); }
+    __device__ __forceinline__ static void st(Ref r, int i, float v) { r[32 * i] = v; }
 };
+// First row of the clauses: right after the variables' rows in shared memory; in a
+// global slab at the next 32-element block, so a warp's clause rows share blocks.
+template <bool G>
+__host__ __device__ inline int row_clause_base(int n) { return G ? (n + 31) & ~31 : n; }
 
 template <int S, typename R>
 __device__ __forceinline__ Row6 load_row(typename R::Ref r) {
@@ -235,7 +244,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             continue;
         }
         const DevInstance I = P.inst[pidx];
-        const int n = I.n, m = I.m;
+        const int n = I.n, m = I.m, cb = row_clause_base<ROWS_G>(n);
         float* const sy = reinterpret_cast<float*>(smem_raw);
         float* const cs = reinterpret_cast<float*>(smem_raw + I.cs_off);
         R rs;
@@ -248,7 +257,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         // initial state: public spins to internal order, a -> log2 a
         const int32_t* const icp = ROWS_G ? I.picperm : I.icperm;  // public -> internal clause
         for (int i = tid; i < n; i += nt) R::st(rs.at(__ldg(I.iperm + i)), 0, G[i]);
-        for (int j = tid; j < m; j += nt) R::st(rs.at(n + __ldg(icp + j)), 0, log2f(G[n + j]));
+        for (int j = tid; j < m; j += nt) R::st(rs.at(cb + __ldg(icp + j)), 0, log2f(G[n + j]));
         if constexpr (!ROWS_G)  // padding slots are read as zeros (the parts form reads counts)
             for (int j = tid; j <= I.nslots; j += nt) cs[j] = 0.0f;
         if (tid == 0) sy[n] = -1.0f;  // sentinel spin: padding literals are always FALSE
@@ -267,7 +276,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 for (int pp = 0; pp < np; pp++) {
                     const int c0 = ld_ro(I.part_c0 + pp), c1 = ld_ro(I.part_c0 + pp + 1);
                     const uint32_t* lp = I.plit + (size_t)(c0 + tid) * K;
-                    typename R::Ref ra = rs.at(n + c0 + tid);
+                    typename R::Ref ra = rs.at(cb + c0 + tid);
                     for (int c = c0 + tid; c < c1; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                         const Row6 o = load_row<S, R>(ra);
                         const float d = part_clause<K>(sm0, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
@@ -306,7 +315,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 return;
             }
             const uint32_t* lp = I.flit + (size_t)tid * K;
-            typename R::Ref ra = rs.at(n + tid);
+            typename R::Ref ra = rs.at(cb + tid);
             for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                 const Row6 o = load_row<S, R>(ra);
                 const float d = fast_clause<K>(sm0, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
@@ -392,7 +401,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     R::st(r, 0, R::ld(r, 2));
                 }
                 for (int c = tid; c < m; c += nt) {
-                    const typename R::Ref r = rs.at(n + c);
+                    const typename R::Ref r = rs.at(cb + c);
                     R::st(r, 0, R::ld(r, 2));
                 }
             }
@@ -451,7 +460,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         // write back the final state in the public layout
         g.sync();
         for (int i = tid; i < n; i += nt) G[i] = R::ld(rs.at(__ldg(I.iperm + i)), 0);
-        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(R::ld(rs.at(n + __ldg(icp + j)), 0));
+        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(R::ld(rs.at(cb + __ldg(icp + j)), 0));
         if (tid == 0) {
             UnitResult r;
             r.time = t; r.hdid = hdid; r.status = status; r.steps = steps; r.attempts = attempts;
