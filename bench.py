@@ -87,7 +87,15 @@ def parse_args():
                     help="maxsat workload: stop every trajectory after this many steps (0: budget only)")
     ap.add_argument("--max-steps", type=int, default=WORKLOAD["maxsteps"],
                     help="per-trajectory step cap (profiling runs use a small one)")
-    return ap.parse_args()
+    ap.add_argument("--n", type=int, default=0,
+                    help="profiling runs: planted instances of this N (M = 4.25 N) instead of "
+                         "N=1000; the bench line then names that workload")
+    args = ap.parse_args()
+    if args.n:
+        m = int(round(4.25 * args.n))
+        WORKLOAD.update(n=args.n, m=m, name=f"planted-3sat-N{args.n}-M{m}-x{args.instances}-inst-"
+                                            f"x{args.traj}-traj")
+    return args
 
 
 def reduce_over_ranks(dist, sums, tmax, device):
