@@ -98,9 +98,9 @@ struct DevicePool {
         AS_CUDA(icperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(cperm.alloc(std::max<size_t>(nc, 1) * 4));
         AS_CUDA(inst.alloc(sizeof(DevInstance) * std::max<size_t>(pk.size(), 1)));
-        // clause-major literal words with shared-memory addressing for the lean FP32
-        // solver, for the instances that fit (bits 0-13 spin byte offset, 14-30 slot
-        // index, 31 sign)
+        // literal words with shared-memory addressing for the lean FP32 solver, for the
+        // instances that fit (bits 0-13 spin byte offset, 14-30 slot index, 31 sign),
+        // blocked by 32 clauses (lean_word_index)
         std::vector<uint32_t> fw;
         std::vector<long long> fw_off;
         for (auto* q : pk) {
@@ -109,12 +109,14 @@ struct DevicePool {
                 fw_off.push_back(-1);
                 continue;
             }
-            fw_off.push_back((long long)fw.size());
+            const size_t f0 = fw.size();
+            fw_off.push_back((long long)f0);
+            fw.resize(f0 + lean_words(q->m, q->k), 0u);
             for (int c = 0; c < q->m; c++)
                 for (int qq = 0; qq < q->k; qq++) {
                     const uint32_t w = q->lit[(size_t)qq * q->mp + c];
                     const uint32_t var = (w >> 16) & 0x7fffu, slot = w & 0xffffu;
-                    fw.push_back((w & 0x80000000u) | (slot << 14) | (4u * var));
+                    fw[f0 + lean_word_index(c, qq, q->k)] = (w & 0x80000000u) | (slot << 14) | (4u * var);
                 }
         }
         AS_CUDA(flit.alloc(std::max<size_t>(fw.size(), 1) * 4));
@@ -129,7 +131,11 @@ struct DevicePool {
                 const PartLayout& L = (*parts)[i];
                 if (L.nparts < 1) continue;
                 poff[i] = {pw.size(), pc.size(), ps.size(), pn.size(), pi.size()};
-                pw.insert(pw.end(), L.words.begin(), L.words.end());
+                const size_t w0 = pw.size();  // clause-major words, blocked by 32 clauses
+                pw.resize(w0 + lean_words(pk[i]->m, pk[i]->k), 0u);
+                for (int c = 0; c < pk[i]->m; c++)
+                    for (int qq = 0; qq < pk[i]->k; qq++)
+                        pw[w0 + lean_word_index(c, qq, pk[i]->k)] = L.words[(size_t)c * pk[i]->k + qq];
                 pc.insert(pc.end(), L.c0.begin(), L.c0.end());
                 ps.insert(ps.end(), L.srow.begin(), L.srow.end());
                 pn.insert(pn.end(), L.cnt.begin(), L.cnt.end());

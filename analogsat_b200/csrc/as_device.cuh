@@ -40,18 +40,19 @@ struct DevInstance {
     int tanh;
     double q, b;
     // Lean FP32 solver layout (solve_kernel_fast), or null when the instance does not
-    // qualify: clause-major literal words flit[m * k + q] that carry shared-memory
-    // addressing -- bit 31 negated literal, bits 14-30 the literal's contribution slot,
-    // bits 0-13 the byte offset of its spin (the spins sit at offset 0 of the dynamic
-    // shared memory, the slots at cs_off, the interleaved RK stage rows at rows_off or
-    // in a global slab).
+    // qualify: literal words flit[lean_word_index(m, q, k)] (blocked by 32 clauses,
+    // as_fast.cuh) that carry shared-memory addressing -- bit 31 negated literal, bits
+    // 14-30 the literal's contribution slot, bits 0-13 the byte offset of its spin (the
+    // spins sit at offset 0 of the dynamic shared memory, the slots at cs_off, the
+    // interleaved RK stage rows at rows_off or, blocked, in a global slab).
     const uint32_t* flit;
     int cs_off, rows_off;
     // Clause parts of the lean kernel's global-rows form (PartLayout in as_problem.h):
-    // words plit[m * k + q] = sign | slot in the part's buffer << 13 | internal variable,
-    // part p's internal clauses [part_c0[p], part_c0[p + 1]), SELL rows part_srow[p *
-    // (nslices + 1) + g], occurrences part_cnt[p * n + v], its own clause order picperm
-    // (public -> internal); nparts = 0 when the instance has no such layout.
+    // words plit[lean_word_index(m, q, k)] = sign | slot in the part's buffer << 13 |
+    // internal variable, part p's internal clauses [part_c0[p], part_c0[p + 1]), SELL
+    // rows part_srow[p * (nslices + 1) + g], occurrences part_cnt[p * n + v], its own
+    // clause order picperm (public -> internal); nparts = 0 when the instance has no
+    // such layout.
     const uint32_t* plit;
     const int32_t* part_c0;
     const int32_t* part_srow;

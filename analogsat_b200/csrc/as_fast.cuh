@@ -13,8 +13,9 @@
 //    shared memory), bits 14-30 the index of its contribution slot, bit 31 the sign.
 //    A spin gather is one mask and one load, a contribution store a shift, a mask, a
 //    scaled add and a store.
-//  * Literal words are clause-major (flit[m * K + q]), so a clause's K words are
-//    loads at immediate offsets from one pointer that advances once per clause.
+//  * Literal words are blocked by 32 clauses ([m / 32][q][m % 32]), so a clause's K
+//    words are loads at immediate offsets from one pointer that advances once per
+//    clause, and a warp's 32 clauses load each word as one 128-byte line.
 //  * The six RK vectors of an element are interleaved, [e][X, K1, K2, K3, K4, K5]
 //    (24 bytes per element): a stage input is one row address and 64-bit loads at
 //    immediate offsets (a 16-lane half-warp at a 24-byte stride covers all 32 banks
@@ -58,6 +59,14 @@ __host__ __device__ inline FastLayout fast_layout(int n, int m, int nslots) {
     L.ok = 4ll * n < 16384 && nslots < (1 << 17);
     return L;
 }
+
+// The lean kernels' literal words are blocked by 32 clauses, [c / 32][q][c % 32]: the
+// 32 consecutive clauses of a warp load word q as one 128-byte line (clause-major words
+// would spread it over 12 or 16 sectors).  lean_words: the words of m clauses, padded.
+__host__ __device__ inline size_t lean_word_index(int c, int q, int k) {
+    return (size_t)(c >> 5) * 32 * k + 32 * q + (c & 31);
+}
+__host__ __device__ inline size_t lean_words(int m, int k) { return (size_t)((m + 31) & ~31) * k; }
 
 __device__ __forceinline__ uint32_t ld_lit(const uint32_t* p) {
     uint32_t v;
@@ -156,7 +165,7 @@ __device__ __forceinline__ float fast_clause(uint32_t sm0, uint32_t cs0, const u
     uint32_t w[K];
     float f[K];
 #pragma unroll
-    for (int q = 0; q < K; q++) w[q] = ld_lit(lp + q);
+    for (int q = 0; q < K; q++) w[q] = ld_lit(lp + 32 * q);
     float km = knorm;
 #pragma unroll
     for (int q = 0; q < K; q++) {
@@ -188,7 +197,7 @@ __device__ __forceinline__ float part_clause(uint32_t sm0, uint32_t cs0, const u
     uint32_t w[K];
     float f[K];
 #pragma unroll
-    for (int q = 0; q < K; q++) w[q] = ld_lit(lp + q);
+    for (int q = 0; q < K; q++) w[q] = ld_lit(lp + 32 * q);
     float km = knorm;
 #pragma unroll
     for (int q = 0; q < K; q++) {
@@ -275,7 +284,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 const int np = I.nparts, ns1 = ((n + 31) >> 5) + 1;
                 for (int pp = 0; pp < np; pp++) {
                     const int c0 = ld_ro(I.part_c0 + pp), c1 = ld_ro(I.part_c0 + pp + 1);
-                    const uint32_t* lp = I.plit + (size_t)(c0 + tid) * K;
+                    const uint32_t* lp = I.plit + lean_word_index(c0 + tid, 0, K);
                     typename R::Ref ra = rs.at(cb + c0 + tid);
                     for (int c = c0 + tid; c < c1; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                         const Row6 o = load_row<S, R>(ra);
@@ -314,7 +323,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 }
                 return;
             }
-            const uint32_t* lp = I.flit + (size_t)tid * K;
+            const uint32_t* lp = I.flit + lean_word_index(tid, 0, K);
             typename R::Ref ra = rs.at(cb + tid);
             for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                 const Row6 o = load_row<S, R>(ra);
@@ -414,12 +423,12 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             g.sync();
             int cnt = 0;
             {
-                const uint32_t* lp = (ROWS_G ? I.plit : I.flit) + (size_t)tid * K;
+                const uint32_t* lp = (ROWS_G ? I.plit : I.flit) + lean_word_index(tid, 0, K);
                 for (int c = tid; c < m; c += nt, lp += (size_t)nt * K) {
                     bool sat = false;
 #pragma unroll
                     for (int q = 0; q < K; q++) {
-                        const uint32_t w = ld_lit(lp + q);
+                        const uint32_t w = ld_lit(lp + 32 * q);
                         const uint32_t sa = ROWS_G ? 4u * (w & 0x1FFFu) : (w & 0x3FFFu);
                         const bool tv = lds(sm0 + sa) > 0.0f;
                         sat |= (w & 0x80000000u) ? !tv : tv;
