@@ -223,6 +223,31 @@ __device__ __forceinline__ float part_clause(uint32_t sm0, uint32_t cs0, const u
     return km * km * kInvLn2;
 }
 
+// Block max of the error ratios, post-processed by thread 0.  The ratios are FP32 and
+// never negative (fmaxf from 0 skips NaN), so their bit patterns order like their values
+// and a warp's max is one integer redux; the max of floats then converted is the FP64
+// max of the converted values, as the general kernel forms it.  red_u is written only
+// here, and a block barrier always separates two calls.
+template <typename F>
+__device__ __forceinline__ double lean_max_then(float em, uint32_t* red_u, double* red_d, F&& fn) {
+    const uint32_t v = __reduce_max_sync(0xffffffffu, __float_as_uint(em));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) red_u[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t x = __reduce_max_sync(0xffffffffu, lane < (int)(blockDim.x >> 5) ? red_u[lane] : 0u);
+        if (lane == 0) red_d[33] = fn((double)__uint_as_float(x));
+    }
+    __syncthreads();
+    return red_d[33];
+}
+
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 // ROWS_G = false: rows, spins and slots in shared memory, words flit.  ROWS_G = true:
 // rows in the CTA's global slab, spins and slots in shared memory, clauses in parts
 // (words plit), each part's contributions summed before the next part reuses the slots.
@@ -232,6 +257,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double red_d[36];
     __shared__ int red_i[33];
+    __shared__ uint32_t red_u[32];
     __shared__ int s_unit, s_flag;
     const Grp<1> g;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -262,6 +288,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         const uint32_t cs0 = sm0 + (uint32_t)I.cs_off;
         float* G = reinterpret_cast<float*>(P.states) + P.unit_state[u];
         const float knorm = (float)ldexp(1.0, -I.k);
+        // the wall-clock deadline (stamped before the launch)
+        const unsigned long long deadline = P.deadline ? *P.deadline : 0ull;
 
         // initial state: public spins to internal order, a -> log2 a
         const int32_t* const icp = ROWS_G ? I.picperm : I.icperm;  // public -> internal clause
@@ -271,6 +299,23 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             for (int j = tid; j <= I.nslots; j += nt) cs[j] = 0.0f;
         if (tid == 0) sy[n] = -1.0f;  // sentinel spin: padding literals are always FALSE
         g.sync();  // the scatter above wrote rows that other threads own in the stage loops
+
+        // The step size after an accepted step (CpuRungeKutta.cpp:252-256) is needed only
+        // from the next step's stage 2 on, so it is formed during the next stage 1, after
+        // the clause loop, by lane 0 of the last warp: that warp has no more clauses than
+        // the first, so the FP64 pow() runs while the first warps finish theirs.
+        double hnext = 1e-9, e_acc = 0.0, h_acc = 0.0;
+        bool h_pending = false;
+        const int pow_tid = nt >= 64 ? nt - 32 : 0;
+        auto settle_h = [&]() {
+            if (h_pending && tid == pow_tid)
+                red_d[34] = e_acc > ck::ERRCON ? __dmul_rn(__dmul_rn(ck::SAFETY, h_acc), pow(e_acc, ck::PGROW))
+                                               : __dmul_rn(5.0, h_acc);
+        };
+        auto take_h = [&]() {
+            if (h_pending) hnext = red_d[34];
+            h_pending = false;
+        };
 
         // One RHS evaluation at stage S (the stage input formed from the rows); the
         // derivative lands in slot S of the rows, or for S == 6 is consumed at once into
@@ -296,7 +341,11 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                             R::st(ra, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT));
                         }
                     }
+                    if constexpr (S == 1)
+                        if (pp + 1 == np) settle_h();
                     g.sync();
+                    if constexpr (S == 1)
+                        if (pp + 1 == np) take_h();
                     // each variable's sum continues from the previous part (kept in slot S,
                     // or for S = 6 in slot 2, whose K2 the stage-6 input has read already)
                     constexpr int SLOT = S < 6 ? S : 2;
@@ -335,7 +384,9 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     R::st(ra, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, d, hT));
                 }
             }
+            if constexpr (S == 1) settle_h();
             g.sync();
+            if constexpr (S == 1) take_h();
             for (int v = tid; v < n; v += nt) {
                 const int g32 = v >> 5;
                 const int r0 = ld_ro(I.srow + g32), r1 = ld_ro(I.srow + g32 + 1);
@@ -354,7 +405,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             }
         };
 
-        double t = 0.0, hnext = 1e-9, hdid = 0.0;
+        double t = 0.0, hdid = 0.0;
         int steps = 0, attempts = 0, rhs = 0, viol = -1, minviol = INT_MAX;
         int status = SAT_UNKNOWN;
 
@@ -375,28 +426,30 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     eval(std::integral_constant<int, 3>{}, hT, h0T, em);
                     eval(std::integral_constant<int, 4>{}, hT, h0T, em);
                     eval(std::integral_constant<int, 5>{}, hT, h0T, em);
+                    // another start's solution (stop-on-first), read now so that the read
+                    // completes during stage 6
+                    int other_solved = 0;
+                    if (tid == 0 && P.stop_on_first) other_solved = ld_relaxed(P.inst_solved + pidx);
                     eval(std::integral_constant<int, 6>{}, hT, h0T, em);
                     rhs += 5;
                     attempts++;
-                    ermax = group_max_then<1>(g, (double)em, red_d, [&](double emax) {
+                    ermax = lean_max_then(em, red_u, red_d, [&](double emax) {
                         const double e = __ddiv_rn(emax, P.eps);
-                        double hn;
-                        if (e <= 1.0)
-                            hn = e > ck::ERRCON ? __dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PGROW))
-                                                : __dmul_rn(5.0, h);
-                        else
-                            hn = fmax(__dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PSHRNK)),
-                                      __dmul_rn(ck::HFACTOR, h));
-                        red_d[34] = hn;
-                        const bool quit = (P.stop_on_first && atomicAdd(P.inst_solved + pidx, 0) != 0) ||
-                                          (P.deadline && globaltimer_ns() >= *P.deadline);
+                        if (e > 1.0)  // rejected: the retry's step size now (accepted: settle_h)
+                            red_d[34] = fmax(__dmul_rn(__dmul_rn(ck::SAFETY, h), pow(e, ck::PSHRNK)),
+                                             __dmul_rn(ck::HFACTOR, h));
+                        const bool quit = other_solved != 0 || (P.deadline && globaltimer_ns() >= deadline);
                         red_d[35] = quit ? 1.0 : 0.0;
                         return e;
                     });
-                    const double hn = red_d[34];
                     if (red_d[35] != 0.0) { interrupted = true; break; }
-                    if (ermax <= 1.0) { hnext = hn; break; }
-                    h = hn;
+                    if (ermax <= 1.0) {
+                        e_acc = ermax;
+                        h_acc = h;
+                        h_pending = true;
+                        break;
+                    }
+                    h = red_d[34];
                     if (__dadd_rn(t, h) == t) { underflow = true; break; }
                 }
                 if (underflow || interrupted) break;
