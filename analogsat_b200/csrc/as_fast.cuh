@@ -150,6 +150,16 @@ template <int S>
 __device__ __forceinline__ float row_input(const Row6& o, float h) {
     return stage_in<S, float>(o.x, o.k1, o.k2, o.k3, o.k4, o.k5, h);
 }
+// Puts the stage-S derivative into its place of a row read for stage S, which then
+// holds what stage S + 1 reads.
+template <int S>
+__device__ __forceinline__ void set_k(Row6& o, float k) {
+    if constexpr (S == 1) o.k1 = k;
+    if constexpr (S == 2) o.k2 = k;
+    if constexpr (S == 3) o.k3 = k;
+    if constexpr (S == 4) o.k4 = k;
+    if constexpr (S == 5) o.k5 = k;
+}
 
 // 1 - c s for a literal word (the sign bit flips s: 1 - (-s) = 1 + s), as clause_phase.
 __device__ __forceinline__ float lit_factor(uint32_t sm0, uint32_t w) {
@@ -317,13 +327,15 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             h_pending = false;
         };
 
-        // One RHS evaluation at stage S (the stage input formed from the rows); the
-        // derivative lands in slot S of the rows, or for S == 6 is consumed at once into
-        // the candidate state (slot 2) and the error norm.
-        auto eval = [&](auto stage, float hT, float h0T, float& em) {
+        // One RHS evaluation at stage S; the derivative lands in slot S of the rows, or
+        // for S == 6 is consumed at once into the candidate state (slot 2) and the error
+        // norm.  The spins' stage input is formed by the variable phase of the stage
+        // before (ready = true; stage 1's by the accepted step's copy), or here.
+        auto eval = [&](auto stage, float hT, float h0T, float& em, bool ready) {
             constexpr int S = decltype(stage)::value;
-            for (int v = tid; v < n; v += nt)
-                sts(sm0 + 4u * (uint32_t)v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
+            if (!ready)
+                for (int v = tid; v < n; v += nt)
+                    sts(sm0 + 4u * (uint32_t)v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
             g.sync();
             if constexpr (ROWS_G) {
                 const int np = I.nparts, ns1 = ((n + 31) >> 5) + 1;
@@ -355,6 +367,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                         const int r0 = ld_ro(I.part_srow + (size_t)pp * ns1 + (v >> 5));
                         uint32_t pa = cs0 + 4u * (uint32_t)(r0 * 32 + (v & 31));
                         const typename R::Ref r = rs.at(v);
+                        Row6 o;  // what the next stage's input (or stage 6) reads, loaded first
+                        if (last) o = load_row<S, R>(r);
                         float sum = pp == 0 ? 0.0f : R::ld(r, SLOT);
 #pragma unroll 4
                         for (int k = 0; k < cnt; k++, pa += 128u) sum = sum + lds(pa);
@@ -362,8 +376,9 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                             R::st(r, SLOT, sum);
                         } else if constexpr (S < 6) {
                             R::st(r, S, sum);
+                            set_k<S>(o, sum);
+                            sts(sm0 + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
                         } else {
-                            const Row6 o = load_row<6, R>(r);
                             em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
                             R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
                         }
@@ -391,14 +406,16 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 const int g32 = v >> 5;
                 const int r0 = ld_ro(I.srow + g32), r1 = ld_ro(I.srow + g32 + 1);
                 uint32_t p = cs0 + 4u * (uint32_t)(r0 * 32 + (v & 31));
+                const typename R::Ref r = rs.at(v);
+                Row6 o = load_row<S, R>(r);  // what the next stage's input (or stage 6) reads
                 float sum = 0.0f;
 #pragma unroll 4
                 for (int k = r0; k < r1; k++, p += 128u) sum = sum + lds(p);
-                const typename R::Ref r = rs.at(v);
                 if constexpr (S < 6) {
                     R::st(r, S, sum);
+                    set_k<S>(o, sum);
+                    sts(sm0 + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
                 } else {
-                    const Row6 o = load_row<6, R>(r);
                     em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
                     R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
                 }
@@ -406,6 +423,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         };
 
         double t = 0.0, hdid = 0.0;
+        bool s1_ready = false;  // the spins hold the accepted state (stage 1's input)
         int steps = 0, attempts = 0, rhs = 0, viol = -1, minviol = INT_MAX;
         int status = SAT_UNKNOWN;
 
@@ -414,23 +432,24 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             int taken = 0;
             for (int b = 0; b < P.batch; b++) {
                 float dummy = 0.0f;
-                eval(std::integral_constant<int, 1>{}, 0.0f, 0.0f, dummy);
+                eval(std::integral_constant<int, 1>{}, 0.0f, 0.0f, dummy, s1_ready);
                 rhs++;
                 const double h0 = hnext;
                 const float h0T = (float)h0;
                 double h = hnext, ermax = 0.0;
+                bool retry = false;  // a retry's stage-2 input uses the smaller step
                 while (true) {
                     const float hT = (float)h;
                     float em = 0.0f;
-                    eval(std::integral_constant<int, 2>{}, hT, h0T, em);
-                    eval(std::integral_constant<int, 3>{}, hT, h0T, em);
-                    eval(std::integral_constant<int, 4>{}, hT, h0T, em);
-                    eval(std::integral_constant<int, 5>{}, hT, h0T, em);
+                    eval(std::integral_constant<int, 2>{}, hT, h0T, em, !retry);
+                    eval(std::integral_constant<int, 3>{}, hT, h0T, em, true);
+                    eval(std::integral_constant<int, 4>{}, hT, h0T, em, true);
+                    eval(std::integral_constant<int, 5>{}, hT, h0T, em, true);
                     // another start's solution (stop-on-first), read now so that the read
                     // completes during stage 6
                     int other_solved = 0;
                     if (tid == 0 && P.stop_on_first) other_solved = ld_relaxed(P.inst_solved + pidx);
-                    eval(std::integral_constant<int, 6>{}, hT, h0T, em);
+                    eval(std::integral_constant<int, 6>{}, hT, h0T, em, true);
                     rhs += 5;
                     attempts++;
                     ermax = lean_max_then(em, red_u, red_d, [&](double emax) {
@@ -450,6 +469,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                         break;
                     }
                     h = red_d[34];
+                    retry = true;
                     if (__dadd_rn(t, h) == t) { underflow = true; break; }
                 }
                 if (underflow || interrupted) break;
@@ -457,11 +477,15 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 t = __dadd_rn(t, h);
                 taken++;
                 // accept: the candidate state (slot 2) becomes the state, each element by
-                // the thread that owns it in the stage loops
+                // the thread that owns it in the stage loops; the spins are also the next
+                // stage 1's input
                 for (int v = tid; v < n; v += nt) {
                     const typename R::Ref r = rs.at(v);
-                    R::st(r, 0, R::ld(r, 2));
+                    const float xn = R::ld(r, 2);
+                    R::st(r, 0, xn);
+                    sts(sm0 + 4u * (uint32_t)v, xn);
                 }
+                s1_ready = true;
                 for (int c = tid; c < m; c += nt) {
                     const typename R::Ref r = rs.at(cb + c);
                     R::st(r, 0, R::ld(r, 2));
