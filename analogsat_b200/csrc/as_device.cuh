@@ -43,7 +43,7 @@ struct DevInstance {
     // qualify: literal words flit[lean_word_index(m, q, k)] (blocked by 32 clauses,
     // as_fast.cuh) that carry shared-memory addressing -- bit 31 negated literal, bits
     // 14-30 the literal's contribution slot, bits 0-13 the byte offset of its spin (the
-    // spins sit at offset 0 of the dynamic shared memory, the slots at cs_off, the
+    // spins sit at the spin base, spin_align-aligned, the slots at cs_off from it, the
     // interleaved RK stage rows at rows_off or, blocked, in a global slab).
     const uint32_t* flit;
     int cs_off, rows_off;

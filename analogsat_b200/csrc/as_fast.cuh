@@ -9,10 +9,10 @@
 // the instructions it executes per clause and stage:
 //
 //  * Literal words carry shared-memory addressing (DevInstance::flit): bits 0-13 the
-//    byte offset of the literal's spin (the spins start at offset 0 of the dynamic
-//    shared memory), bits 14-30 the index of its contribution slot, bit 31 the sign.
-//    A spin gather is one mask and one load, a contribution store a shift, a mask, a
-//    scaled add and a store.
+//    byte offset of the literal's spin from the spin base (aligned to a power of two
+//    at least the spins' size, so base | offset is the address), bits 14-30 the index
+//    of its contribution slot, bit 31 the sign.  A spin gather is one logic operation
+//    and one load, a contribution store a shift, a mask, a scaled add and a store.
 //  * Literal words are blocked by 32 clauses ([m / 32][q][m % 32]), so a clause's K
 //    words are loads at immediate offsets from one pointer that advances once per
 //    clause, and a warp's 32 clauses load each word as one 128-byte line.
@@ -44,6 +44,14 @@ namespace asb {
 // Shared-memory byte offsets of the lean layout for an instance, and whether its
 // literal words can carry them (spin offsets below 16 KB, slot indices below 2^17).
 // bytes: shared memory with the rows on chip; bytes_g: without them (ROWS_G).
+// The all-shared form places the spins at a shared address aligned to spin_align (the
+// smallest power of two >= their bytes), so a spin's address is that base OR the byte
+// offset of its literal word: one logic operation.  bytes counts the worst-case padding.
+__host__ __device__ inline uint32_t spin_align(int n) {
+    uint32_t a = 128;
+    while (a < 4u * (uint32_t)(n + 1)) a <<= 1;
+    return a;
+}
 struct FastLayout {
     bool ok = false;
     int cs_off = 0, rows_off = 0;
@@ -54,7 +62,7 @@ __host__ __device__ inline FastLayout fast_layout(int n, int m, int nslots) {
     L.cs_off = ((4 * (n + 1)) + 127) / 128 * 128;  // a multiple of 128 B keeps slot banks
     const long long cs_end = (long long)L.cs_off + 4ll * (nslots + 1);
     L.rows_off = (int)((cs_end + 15) / 16 * 16);
-    L.bytes = (size_t)L.rows_off + 24ull * (size_t)(n + m);
+    L.bytes = (size_t)L.rows_off + 24ull * (size_t)(n + m) + spin_align(n) - 16;
     L.bytes_g = (size_t)L.rows_off;
     L.ok = 4ll * n < 16384 && nslots < (1 << 17);
     return L;
@@ -162,8 +170,8 @@ __device__ __forceinline__ void set_k(Row6& o, float k) {
 }
 
 // 1 - c s for a literal word (the sign bit flips s: 1 - (-s) = 1 + s), as clause_phase.
-__device__ __forceinline__ float lit_factor(uint32_t sm0, uint32_t w) {
-    const float s = lds(sm0 + (w & 0x3FFFu));
+__device__ __forceinline__ float lit_factor(uint32_t sb, uint32_t mask, uint32_t w) {
+    const float s = lds(sb | (w & mask));
     return 1.0f - __int_as_float(__float_as_int(s) ^ (int)(w & 0x80000000u));
 }
 
@@ -171,7 +179,8 @@ __device__ __forceinline__ float lit_factor(uint32_t sm0, uint32_t w) {
 // K_m, the leave-one-out products in CpuProdWrapper order, contributions into their
 // slots; returns du_m = K_m^2 / ln 2.  Same operations as clause_phase<float, true, K>.
 template <int K>
-__device__ __forceinline__ float fast_clause(uint32_t sm0, uint32_t cs0, const uint32_t* lp, float am, float knorm) {
+__device__ __forceinline__ float fast_clause(uint32_t sb, uint32_t mask, uint32_t cs0, const uint32_t* lp, float am,
+                                             float knorm) {
     uint32_t w[K];
     float f[K];
 #pragma unroll
@@ -179,7 +188,7 @@ __device__ __forceinline__ float fast_clause(uint32_t sm0, uint32_t cs0, const u
     float km = knorm;
 #pragma unroll
     for (int q = 0; q < K; q++) {
-        f[q] = lit_factor(sm0, w[q]);
+        f[q] = lit_factor(sb, mask, w[q]);
         km = km * f[q];
     }
     const float r = (km * knorm) * am;
@@ -290,12 +299,15 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         }
         const DevInstance I = P.inst[pidx];
         const int n = I.n, m = I.m, cb = row_clause_base<ROWS_G>(n);
-        float* const sy = reinterpret_cast<float*>(smem_raw);
-        float* const cs = reinterpret_cast<float*>(smem_raw + I.cs_off);
+        // spin base: aligned in the all-shared form (spin_align), the start otherwise
+        const uint32_t mask = ROWS_G ? 0u : spin_align(n) - 1u;
+        const uint32_t sb = ROWS_G ? sm0 : (sm0 + mask) & ~mask;
+        float* const sy = reinterpret_cast<float*>(smem_raw + (sb - sm0));
+        float* const cs = reinterpret_cast<float*>(smem_raw + (sb - sm0) + I.cs_off);
         R rs;
         if constexpr (ROWS_G) rs.base = reinterpret_cast<float*>(P.slab) + (long long)blockIdx.x * P.slab_stride;
-        else rs.base = sm0 + (uint32_t)I.rows_off;
-        const uint32_t cs0 = sm0 + (uint32_t)I.cs_off;
+        else rs.base = sb + (uint32_t)I.rows_off;
+        const uint32_t cs0 = sb + (uint32_t)I.cs_off;
         float* G = reinterpret_cast<float*>(P.states) + P.unit_state[u];
         const float knorm = (float)ldexp(1.0, -I.k);
         // the wall-clock deadline (stamped before the launch)
@@ -335,7 +347,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             constexpr int S = decltype(stage)::value;
             if (!ready)
                 for (int v = tid; v < n; v += nt)
-                    sts(sm0 + 4u * (uint32_t)v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
+                    sts(sb + 4u * (uint32_t)v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
             g.sync();
             if constexpr (ROWS_G) {
                 const int np = I.nparts, ns1 = ((n + 31) >> 5) + 1;
@@ -345,7 +357,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     typename R::Ref ra = rs.at(cb + c0 + tid);
                     for (int c = c0 + tid; c < c1; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                         const Row6 o = load_row<S, R>(ra);
-                        const float d = part_clause<K>(sm0, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+                        const float d = part_clause<K>(sb, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
                         if constexpr (S < 6) {
                             R::st(ra, S, d);
                         } else {
@@ -377,7 +389,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                         } else if constexpr (S < 6) {
                             R::st(r, S, sum);
                             set_k<S>(o, sum);
-                            sts(sm0 + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
+                            sts(sb + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
                         } else {
                             em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
                             R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
@@ -391,7 +403,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             typename R::Ref ra = rs.at(cb + tid);
             for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                 const Row6 o = load_row<S, R>(ra);
-                const float d = fast_clause<K>(sm0, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+                const float d = fast_clause<K>(sb, mask, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
                 if constexpr (S < 6) {
                     R::st(ra, S, d);
                 } else {
@@ -414,7 +426,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 if constexpr (S < 6) {
                     R::st(r, S, sum);
                     set_k<S>(o, sum);
-                    sts(sm0 + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
+                    sts(sb + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
                 } else {
                     em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
                     R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
@@ -483,7 +495,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     const typename R::Ref r = rs.at(v);
                     const float xn = R::ld(r, 2);
                     R::st(r, 0, xn);
-                    sts(sm0 + 4u * (uint32_t)v, xn);
+                    sts(sb + 4u * (uint32_t)v, xn);
                 }
                 s1_ready = true;
                 for (int c = tid; c < m; c += nt) {
@@ -496,7 +508,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             if (interrupted) { status = SAT_ODE_INTERRUPTED; break; }
 
             // CpuSat::GetClauseViolationCount on the accepted state
-            for (int v = tid; v < n; v += nt) sts(sm0 + 4u * (uint32_t)v, R::ld(rs.at(v), 0));
+            for (int v = tid; v < n; v += nt) sts(sb + 4u * (uint32_t)v, R::ld(rs.at(v), 0));
             g.sync();
             int cnt = 0;
             {
@@ -506,8 +518,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
 #pragma unroll
                     for (int q = 0; q < K; q++) {
                         const uint32_t w = ld_lit(lp + 32 * q);
-                        const uint32_t sa = ROWS_G ? 4u * (w & 0x1FFFu) : (w & 0x3FFFu);
-                        const bool tv = lds(sm0 + sa) > 0.0f;
+                        const uint32_t sa = ROWS_G ? sb + 4u * (w & 0x1FFFu) : (sb | (w & mask));
+                        const bool tv = lds(sa) > 0.0f;
                         sat |= (w & 0x80000000u) ? !tv : tv;
                     }
                     cnt += sat ? 0 : 1;
