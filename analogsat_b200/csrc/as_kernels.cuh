@@ -529,14 +529,15 @@ __global__ void __launch_bounds__(BT) rhs_batch_kernel(DevInstance I, const T* _
 //
 // Data movement: two consecutive public states (contiguous in HBM) arrive in a shared
 // staging buffer with one 1-D bulk copy (cp.async.bulk, mbarrier completion) that is
-// issued one pair ahead; the < 16-byte ragged ends of a row pair that does not start
-// on a 16-byte boundary are fetched with plain loads.  The kernel then works in the
+// issued one pair ahead by lane 0 of the last warp; the < 16-byte ragged ends of a row
+// pair that does not start on a 16-byte boundary are fetched with plain loads.  The kernel then works in the
 // public layout in place: a_m is read from and da_m written to its public position
 // (the pair packing makes the 32 clauses of a warp hit 32 different banks there), ds
 // is scattered to the public spin positions, and the finished pair leaves with one
 // bulk store (when dxdt and x are congruent mod 16 bytes; plain coalesced stores
 // otherwise).  Two staging buffers alternate: pair i is stored from one while pair
-// i+1 lands in the other.  A wait that does not complete within two seconds (it
+// i+1 lands in the other.  Two barriers per pair: one after the clause phase, one after
+// the variable phase, which also permutes the next pair's spins (its buffer has landed).  A wait that does not complete within two seconds (it
 // cannot, short of a broken device) turns every output of the CTA's remaining pairs
 // into NaN and sets *status to 1 instead of hanging.
 // Shared layout: 2 mbarriers | staging[2] (2 stride + 3 floats each) | sy2 | cs2.
@@ -671,62 +672,60 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
         vp[i] = v < n ? __ldg(I.perm + v) : 0;
         vrows[i] = v < n ? (uint32_t)ld_ro(I.srow + (v >> 5)) | ((uint32_t)ld_ro(I.srow + (v >> 5) + 1) << 16) : 0u;
     }
+    if (tid == 0) sy[n] = f2(-1.0f);
     __syncthreads();
-    // Copy of pair q into buffer b: thread 0 starts the bulk part; threads 0..5 load
-    // the ragged floats into rag (stored into the buffer at the top of the iteration
-    // that consumes it).
-    float rag = 0.0f;
-    int rag_at = -1;  // float index into stg0 (buffer offset included), or -1
+    // All bulk copies and stores are issued by lane 0 of the last warp (IO), so that the
+    // store -> reuse wait falls on a warp with no more clauses than the first.  Copy of
+    // pair q into buffer b: IO starts the bulk part; after it, lanes 0..5 of the same
+    // warp load the < 16-byte ragged ends and store them into the buffer (positions the
+    // bulk copy does not write).  The buffer's previous pair has left it by then: IO
+    // waited for its bulk store to read out, and __syncwarp orders the lanes after it.
+    constexpr int IO = BT - 32;
+    const bool io_warp = tid >= IO;
     auto issue = [&](int q, int b) {
         const PairCopy c(x, q, ntraj, stride);
         float* dst = stg0 + (size_t)b * sf;
-        if (tid == 0) {
+        if (tid == IO) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive_tx(bar + b, (uint32_t)c.nb * 4u);
             if (c.nb > 0) bulk_load(dst + c.off + c.head, c.src + c.head, (uint32_t)c.nb * 4u, bar + b);
         }
-        if (tid < 6) {
-            const int e = c.ragged(tid);
-            rag_at = e >= 0 ? b * (int)sf + c.off + e : -1;
-            if (e >= 0) rag = __ldg(c.src + e);
+        if ((unsigned)(tid - IO) < 6u) {  // lanes 0..5 of the IO warp
+            const int e = c.ragged(tid - IO);
+            if (e >= 0) dst[c.off + e] = __ldg(c.src + e);
         }
     };
-    issue(pr, 0);
-    uint32_t parity = 0;  // bit b: phase parity expected next on bar[b]
-    for (int it = 0; pr < npairs; pr += G, it++) {
+    // Spins of the pair in buffer b into internal order, interleaved.
+    auto permute = [&](int q, int b) {
+        const PairCopy c(x, q, ntraj, stride);
+        const float* A0 = stg0 + (size_t)b * sf + c.off;
+        const float* A1 = 2 * q + 1 < ntraj ? A0 + stride : A0;
+#pragma unroll
+        for (int i = 0; i < VPT; i++)
+            if (tid + i * BT < n) sy[tid + i * BT] = make_float2(A0[vp[i]], A1[vp[i]]);
+    };
+    uint32_t parity = 0;   // bit b: phase parity expected next on bar[b]
+    uint32_t pending = 1;  // bit b: a copy into buffer b not yet waited for (same in all threads)
+    if (io_warp) issue(pr, 0);
+    if (pr + G < npairs) {
+        if (io_warp) issue(pr + G, 1);
+        pending |= 2u;
+    }
+    bool ok = mbar_wait_for(bar, 0, kWaitNs);
+    parity ^= 1u;
+    pending &= ~1u;
+    __syncthreads();  // the ragged ends stored by the IO warp
+    permute(pr, 0);
+    bool failed = __syncthreads_or(!ok);
+    // Per pair: clause phase | barrier | next pair's copy waited for | variable phase of
+    // this pair and spin permutation of the next (independent work in one phase) |
+    // barrier + timeout vote | this pair stored, the pair after next copied in.
+    for (int it = 0; !failed && pr < npairs; pr += G, it++) {
         const int b = it & 1;
-        if (rag_at >= 0) stg0[rag_at] = rag;
-        rag_at = -1;
-        const bool ok = mbar_wait_for(bar + b, (parity >> b) & 1u, kWaitNs);
-        if (__syncthreads_or(!ok)) {
-            mbar_wait_for(bar + b, (parity >> b) & 1u, kWaitNs);  // let a late copy land
-            if (tid == 0) {
-                bulk_wait_all();
-                atomicExch(status, 1);
-            }
-            const float nan = __int_as_float(0x7fc00000);
-            for (; pr < npairs; pr += G) {
-                const long long cnt = (2 * pr + 1 < ntraj ? 2 : 1) * stride;
-                for (long long e = tid; e < cnt; e += BT) dxdt[(long long)(2 * pr) * stride + e] = nan;
-            }
-            return;
-        }
-        parity ^= 1u << b;
         const bool two = 2 * pr + 1 < ntraj;
         const PairCopy cur(x, pr, ntraj, stride);
         float* S0 = stg0 + (size_t)b * sf + cur.off;
         float* S1 = two ? S0 + stride : S0;
-        // spins into internal order, interleaved
-#pragma unroll
-        for (int i = 0; i < VPT; i++)
-            if (tid + i * BT < n) sy[tid + i * BT] = make_float2(S0[vp[i]], S1[vp[i]]);
-        if (tid == 0) sy[n] = f2(-1.0f);
-        __syncthreads();
-        if (pr + G < npairs) {
-            // the other buffer held pair pr - G: its bulk store must have read it out
-            if (tid == 0 && bulk_out) bulk_wait_read();
-            issue(pr + G, b ^ 1);
-        }
         // clause phase: a_m in, da_m out at the public clause position
 #pragma unroll
         for (int i = 0; i < CPT; i++) {
@@ -774,6 +773,13 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
             }
         }
         __syncthreads();
+        const bool more = pr + G < npairs;
+        ok = true;
+        if (more) {
+            ok = mbar_wait_for(bar + (b ^ 1), (parity >> (b ^ 1)) & 1u, kWaitNs);
+            parity ^= 1u << (b ^ 1);
+            pending &= ~(1u << (b ^ 1));
+        }
         // var phase: ds_i to the public spin position
 #pragma unroll
         for (int i = 0; i < VPT; i++) {
@@ -787,22 +793,56 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
             S0[vp[i]] = sum.x;
             S1[vp[i]] = sum.y;
         }
+        // the next pair's spins (its buffer is the other one; sy is free: this pair's
+        // clause phase has read it)
+        if (more) permute(pr + G, b ^ 1);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // results -> bulk store
-        __syncthreads();
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
         float* D = dxdt + (long long)(2 * pr) * stride;
         if (bulk_out) {
-            if (tid == 0 && cur.nb > 0) bulk_store(D + cur.head, S0 + cur.head, (uint32_t)cur.nb * 4u);
-            if (tid < 6) {
-                const int e = cur.ragged(tid);
+            if (tid == IO && cur.nb > 0) bulk_store(D + cur.head, S0 + cur.head, (uint32_t)cur.nb * 4u);
+            if ((unsigned)(tid - IO) < 6u) {
+                const int e = cur.ragged(tid - IO);
                 if (e >= 0) D[e] = S0[e];
             }
         } else {
             for (int e = tid; e < cur.cnt; e += BT) D[e] = S0[e];
+            __syncthreads();  // the buffer is read out before the copy into it
         }
-        // no barrier here: the next writes to this buffer, sy and cs all come after
-        // the next iteration's barriers
+        if (pr + 2 * G < npairs) {
+            // this buffer takes the pair after next once its store has read it out
+            if (io_warp) {
+                if (tid == IO && bulk_out) bulk_wait_read();
+                __syncwarp();
+                issue(pr + 2 * G, b);
+            }
+            pending |= 1u << b;
+        }
+        // no barrier here: the next writes to this buffer (the copy above, after the
+        // store's read), to sy (next variable phase) and to cs (next clause phase) all
+        // come after the next barriers
     }
-    if (tid == 0) bulk_wait_all();
+    if (!failed) {
+        if (tid == IO) bulk_wait_all();
+        return;
+    }
+    // a copy did not land within the limit (it cannot, short of a broken device): let
+    // the copies still in flight land, wait for this CTA's stores, flag the error and
+    // turn every output of the CTA's remaining pairs into NaN
+    for (int b = 0; b < 2; b++)
+        if (pending & (1u << b)) mbar_wait_for(bar + b, (parity >> b) & 1u, kWaitNs);
+    if (tid == IO) {
+        bulk_wait_all();
+        atomicExch(status, 1);
+    }
+    const float nan = __int_as_float(0x7fc00000);
+    for (; pr < npairs; pr += G) {
+        const long long cnt = (2 * pr + 1 < ntraj ? 2 : 1) * stride;
+        for (long long e = tid; e < cnt; e += BT) dxdt[(long long)(2 * pr) * stride + e] = nan;
+    }
 }
 
 // Exact unsat counts of many states: one CTA per state.
