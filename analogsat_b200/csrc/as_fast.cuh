@@ -154,6 +154,21 @@ __device__ __forceinline__ Row6 load_row(typename R::Ref r) {
     }
     return o;
 }
+// A clause row at stage 1: after an accepted step its new state still sits in slot 2
+// (the accepted step's copy of the clause rows is done here, by the owning thread,
+// where the row is read anyway).
+template <int S, typename R>
+__device__ __forceinline__ Row6 load_clause_row(typename R::Ref r, bool from_candidate) {
+    if constexpr (S == 1) {
+        if (from_candidate) {
+            Row6 o;
+            o.x = R::ld(r, 2);
+            R::st(r, 0, o.x);
+            return o;
+        }
+    }
+    return load_row<S, R>(r);
+}
 template <int S>
 __device__ __forceinline__ float row_input(const Row6& o, float h) {
     return stage_in<S, float>(o.x, o.k1, o.k2, o.k3, o.k4, o.k5, h);
@@ -356,7 +371,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     const uint32_t* lp = I.plit + lean_word_index(c0 + tid, 0, K);
                     typename R::Ref ra = rs.at(cb + c0 + tid);
                     for (int c = c0 + tid; c < c1; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
-                        const Row6 o = load_row<S, R>(ra);
+                        const Row6 o = load_clause_row<S, R>(ra, ready);
                         const float d = part_clause<K>(sb, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
                         if constexpr (S < 6) {
                             R::st(ra, S, d);
@@ -374,26 +389,50 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     // or for S = 6 in slot 2, whose K2 the stage-6 input has read already)
                     constexpr int SLOT = S < 6 ? S : 2;
                     const bool last = pp + 1 == np;
-                    for (int v = tid; v < n; v += nt) {
-                        const int cnt = (int)I.part_cnt[(size_t)pp * n + v];
-                        const int r0 = ld_ro(I.part_srow + (size_t)pp * ns1 + (v >> 5));
-                        uint32_t pa = cs0 + 4u * (uint32_t)(r0 * 32 + (v & 31));
+                    // What a variable needs from L2 (occurrence count, SELL row, its row for
+                    // the next stage's input or stage 6, the sum so far), then its sum over
+                    // the part's slots; two variables at a time, both loaded first, so the
+                    // L2 latencies overlap.
+                    struct VarIn {
+                        int cnt, r0;
+                        float sum;
+                        Row6 o;
+                    };
+                    auto var_load = [&](int v) {
+                        VarIn a;
+                        a.cnt = (int)I.part_cnt[(size_t)pp * n + v];
+                        a.r0 = ld_ro(I.part_srow + (size_t)pp * ns1 + (v >> 5));
                         const typename R::Ref r = rs.at(v);
-                        Row6 o;  // what the next stage's input (or stage 6) reads, loaded first
-                        if (last) o = load_row<S, R>(r);
-                        float sum = pp == 0 ? 0.0f : R::ld(r, SLOT);
+                        if (last) a.o = load_row<S, R>(r);
+                        a.sum = pp == 0 ? 0.0f : R::ld(r, SLOT);
+                        return a;
+                    };
+                    auto var_sum = [&](int v, const VarIn& a) {
+                        uint32_t pa = cs0 + 4u * (uint32_t)(a.r0 * 32 + (v & 31));
+                        float sum = a.sum;
 #pragma unroll 4
-                        for (int k = 0; k < cnt; k++, pa += 128u) sum = sum + lds(pa);
+                        for (int k = 0; k < a.cnt; k++, pa += 128u) sum = sum + lds(pa);
+                        const typename R::Ref r = rs.at(v);
                         if (!last) {
                             R::st(r, SLOT, sum);
                         } else if constexpr (S < 6) {
+                            Row6 o = a.o;
                             R::st(r, S, sum);
                             set_k<S>(o, sum);
                             sts(sb + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
                         } else {
+                            const Row6& o = a.o;
                             em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
                             R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
                         }
+                    };
+                    for (int v = tid; v < n; v += 2 * nt) {
+                        const bool two = v + nt < n;
+                        const VarIn a = var_load(v);
+                        VarIn b2;
+                        if (two) b2 = var_load(v + nt);
+                        var_sum(v, a);
+                        if (two) var_sum(v + nt, b2);
                     }
                     if (!last) g.sync();  // the next part's clauses reuse the slots
                 }
@@ -402,7 +441,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             const uint32_t* lp = I.flit + lean_word_index(tid, 0, K);
             typename R::Ref ra = rs.at(cb + tid);
             for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
-                const Row6 o = load_row<S, R>(ra);
+                const Row6 o = load_clause_row<S, R>(ra, ready);
                 const float d = fast_clause<K>(sb, mask, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
                 if constexpr (S < 6) {
                     R::st(ra, S, d);
@@ -435,7 +474,9 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         };
 
         double t = 0.0, hdid = 0.0;
-        bool s1_ready = false;  // the spins hold the accepted state (stage 1's input)
+        // after an accepted step: the spins hold its state (stage 1's input) and the clause
+        // rows' state is still in slot 2 until the next stage 1 moves it
+        bool s1_ready = false;
         int steps = 0, attempts = 0, rhs = 0, viol = -1, minviol = INT_MAX;
         int status = SAT_UNKNOWN;
 
@@ -445,6 +486,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             for (int b = 0; b < P.batch; b++) {
                 float dummy = 0.0f;
                 eval(std::integral_constant<int, 1>{}, 0.0f, 0.0f, dummy, s1_ready);
+                s1_ready = false;  // the clause rows' copy is done
                 rhs++;
                 const double h0 = hnext;
                 const float h0T = (float)h0;
@@ -490,7 +532,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 taken++;
                 // accept: the candidate state (slot 2) becomes the state, each element by
                 // the thread that owns it in the stage loops; the spins are also the next
-                // stage 1's input
+                // stage 1's input.  The clause rows follow in that stage's clause loop.
                 for (int v = tid; v < n; v += nt) {
                     const typename R::Ref r = rs.at(v);
                     const float xn = R::ld(r, 2);
@@ -498,10 +540,6 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     sts(sb + 4u * (uint32_t)v, xn);
                 }
                 s1_ready = true;
-                for (int c = tid; c < m; c += nt) {
-                    const typename R::Ref r = rs.at(cb + c);
-                    R::st(r, 0, R::ld(r, 2));
-                }
             }
             if (underflow) { status = SAT_UNDERFLOW; break; }
             steps += taken;
@@ -558,7 +596,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         // write back the final state in the public layout
         g.sync();
         for (int i = tid; i < n; i += nt) G[i] = R::ld(rs.at(__ldg(I.iperm + i)), 0);
-        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(R::ld(rs.at(cb + __ldg(icp + j)), 0));
+        for (int j = tid; j < m; j += nt) G[n + j] = exp2f(R::ld(rs.at(cb + __ldg(icp + j)), s1_ready ? 2 : 0));
         if (tid == 0) {
             UnitResult r;
             r.time = t; r.hdid = hdid; r.status = status; r.steps = steps; r.attempts = attempts;
