@@ -116,7 +116,10 @@ struct DevicePool {
                 for (int qq = 0; qq < q->k; qq++) {
                     const uint32_t w = q->lit[(size_t)qq * q->mp + c];
                     const uint32_t var = (w >> 16) & 0x7fffu, slot = w & 0xffffu;
-                    fw[f0 + lean_word_index(c, qq, q->k)] = (w & 0x80000000u) | (slot << 14) | (4u * var);
+                    // a negated literal addresses the negated spin copy, which follows
+                    // the N + 1 spins (sentinel included)
+                    const uint32_t so = 4u * var + ((w & 0x80000000u) ? 4u * (uint32_t)(q->n + 1) : 0u);
+                    fw[f0 + lean_word_index(c, qq, q->k)] = (w & 0x80000000u) | (slot << 14) | so;
                 }
         }
         AS_CUDA(flit.alloc(std::max<size_t>(fw.size(), 1) * 4));
@@ -176,6 +179,7 @@ struct DevicePool {
                 d.flit = fo >= 0 ? flit.as<uint32_t>() + fo : nullptr;
                 d.cs_off = L.cs_off;
                 d.rows_off = L.rows_off;
+                d.cs_off_g = L.cs_off_g;
                 const size_t i = host_inst.size();
                 const PartLayout* PL = parts && i < parts->size() ? &(*parts)[i] : nullptr;
                 d.nparts = PL ? PL->nparts : 0;
@@ -259,7 +263,7 @@ const std::vector<Variant>& variants() {
 size_t solver_smem(const Variant& v, const PackedProblem& q) {
     if (v.lean) {
         const FastLayout L = fast_layout(q.n, q.m, q.nslots);
-        return v.gs ? (size_t)L.cs_off + 4 * (size_t)(q.lean_part_slots + 1) : L.bytes;
+        return v.gs ? (size_t)L.cs_off_g + 4 * (size_t)(q.lean_part_slots + 1) : L.bytes;
     }
     if (v.gs) return 0;
     return solve_smem_values(q.n, q.m, q.nslots) * v.bytes_per_value;
@@ -807,7 +811,7 @@ int32_t as_solver_create(const as_problem* const* problems, int32_t num_problems
             for (int np = 1; np <= 4; np++) {
                 PartLayout PL;
                 if (!pack_parts(hp, q, np, PL)) break;
-                if ((size_t)L.cs_off + 4 * (size_t)(PL.max_slots + 1) <= s->smem_limit) {
+                if ((size_t)L.cs_off_g + 4 * (size_t)(PL.max_slots + 1) <= s->smem_limit) {
                     q.lean_parts = np;
                     q.lean_part_slots = PL.max_slots;
                     s->parts[i] = std::move(PL);

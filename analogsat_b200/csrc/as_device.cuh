@@ -46,7 +46,7 @@ struct DevInstance {
     // spins sit at the spin base, spin_align-aligned, the slots at cs_off from it, the
     // interleaved RK stage rows at rows_off or, blocked, in a global slab).
     const uint32_t* flit;
-    int cs_off, rows_off;
+    int cs_off, rows_off, cs_off_g;  // cs_off_g: the global-rows form's slots (one spin copy)
     // Clause parts of the lean kernel's global-rows form (PartLayout in as_problem.h):
     // words plit[lean_word_index(m, q, k)] = sign | slot in the part's buffer << 13 |
     // internal variable, part p's internal clauses [part_c0[p], part_c0[p + 1]), SELL

@@ -44,27 +44,30 @@ namespace asb {
 // Shared-memory byte offsets of the lean layout for an instance, and whether its
 // literal words can carry them (spin offsets below 16 KB, slot indices below 2^17).
 // bytes: shared memory with the rows on chip; bytes_g: without them (ROWS_G).
-// The all-shared form places the spins at a shared address aligned to spin_align (the
-// smallest power of two >= their bytes), so a spin's address is that base OR the byte
-// offset of its literal word: one logic operation.  bytes counts the worst-case padding.
+// The all-shared form holds the spins twice, s_0..s_N (s_N the sentinel) and then
+// -s_0..-s_N, so a negated literal's word points at its negated spin and a gather needs
+// no sign flip; both copies sit at a shared address aligned to spin_align (the smallest
+// power of two >= their bytes), so a spin's address is that base OR the byte offset of
+// its literal word: one logic operation.  bytes counts the worst-case padding.  The
+// global-rows form holds one copy; its slots start at cs_off_g.
 __host__ __device__ inline uint32_t spin_align(int n) {
     uint32_t a = 128;
-    while (a < 4u * (uint32_t)(n + 1)) a <<= 1;
+    while (a < 8u * (uint32_t)(n + 1)) a <<= 1;
     return a;
 }
 struct FastLayout {
     bool ok = false;
-    int cs_off = 0, rows_off = 0;
-    size_t bytes = 0, bytes_g = 0;
+    int cs_off = 0, rows_off = 0, cs_off_g = 0;
+    size_t bytes = 0;
 };
 __host__ __device__ inline FastLayout fast_layout(int n, int m, int nslots) {
     FastLayout L;
-    L.cs_off = ((4 * (n + 1)) + 127) / 128 * 128;  // a multiple of 128 B keeps slot banks
+    L.cs_off = ((8 * (n + 1)) + 127) / 128 * 128;  // a multiple of 128 B keeps slot banks
+    L.cs_off_g = ((4 * (n + 1)) + 127) / 128 * 128;
     const long long cs_end = (long long)L.cs_off + 4ll * (nslots + 1);
     L.rows_off = (int)((cs_end + 15) / 16 * 16);
     L.bytes = (size_t)L.rows_off + 24ull * (size_t)(n + m) + spin_align(n) - 16;
-    L.bytes_g = (size_t)L.rows_off;
-    L.ok = 4ll * n < 16384 && nslots < (1 << 17);
+    L.ok = 8ll * (n + 1) <= 16384 && nslots < (1 << 17);
     return L;
 }
 
@@ -186,8 +189,7 @@ __device__ __forceinline__ void set_k(Row6& o, float k) {
 
 // 1 - c s for a literal word (the sign bit flips s: 1 - (-s) = 1 + s), as clause_phase.
 __device__ __forceinline__ float lit_factor(uint32_t sb, uint32_t mask, uint32_t w) {
-    const float s = lds(sb | (w & mask));
-    return 1.0f - __int_as_float(__float_as_int(s) ^ (int)(w & 0x80000000u));
+    return 1.0f - lds(sb | (w & mask));  // the word points at -s for a negated literal
 }
 
 // Clause phase of one clause (K literals, FP32, log-space weights): spin gathers,
@@ -318,11 +320,18 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         const uint32_t mask = ROWS_G ? 0u : spin_align(n) - 1u;
         const uint32_t sb = ROWS_G ? sm0 : (sm0 + mask) & ~mask;
         float* const sy = reinterpret_cast<float*>(smem_raw + (sb - sm0));
-        float* const cs = reinterpret_cast<float*>(smem_raw + (sb - sm0) + I.cs_off);
+        const int cso = ROWS_G ? I.cs_off_g : I.cs_off;
+        float* const cs = reinterpret_cast<float*>(smem_raw + (sb - sm0) + cso);
         R rs;
         if constexpr (ROWS_G) rs.base = reinterpret_cast<float*>(P.slab) + (long long)blockIdx.x * P.slab_stride;
         else rs.base = sb + (uint32_t)I.rows_off;
-        const uint32_t cs0 = sb + (uint32_t)I.cs_off;
+        const uint32_t cs0 = sb + (uint32_t)cso;
+        // the all-shared form's second, negated spin copy: spin v also at sneg + 4 v
+        const uint32_t sneg = sb + 4u * (uint32_t)(n + 1);
+        auto put_spin = [&](int v, float val) {
+            sts(sb + 4u * (uint32_t)v, val);
+            if constexpr (!ROWS_G) sts(sneg + 4u * (uint32_t)v, -val);
+        };
         float* G = reinterpret_cast<float*>(P.states) + P.unit_state[u];
         const float knorm = (float)ldexp(1.0, -I.k);
         // the wall-clock deadline (stamped before the launch)
@@ -334,7 +343,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         for (int j = tid; j < m; j += nt) R::st(rs.at(cb + __ldg(icp + j)), 0, log2f(G[n + j]));
         if constexpr (!ROWS_G)  // padding slots are read as zeros (the parts form reads counts)
             for (int j = tid; j <= I.nslots; j += nt) cs[j] = 0.0f;
-        if (tid == 0) sy[n] = -1.0f;  // sentinel spin: padding literals are always FALSE
+        if (tid == 0) put_spin(n, -1.0f);  // sentinel spin: padding literals are always FALSE
         g.sync();  // the scatter above wrote rows that other threads own in the stage loops
 
         // The step size after an accepted step (CpuRungeKutta.cpp:252-256) is needed only
@@ -362,7 +371,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             constexpr int S = decltype(stage)::value;
             if (!ready)
                 for (int v = tid; v < n; v += nt)
-                    sts(sb + 4u * (uint32_t)v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
+                    put_spin(v, row_input<S>(load_row<S, R>(rs.at(v)), hT));
             g.sync();
             if constexpr (ROWS_G) {
                 const int np = I.nparts, ns1 = ((n + 31) >> 5) + 1;
@@ -410,7 +419,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     auto var_sum = [&](int v, const VarIn& a) {
                         uint32_t pa = cs0 + 4u * (uint32_t)(a.r0 * 32 + (v & 31));
                         float sum = a.sum;
-#pragma unroll 4
+#pragma unroll 8
                         for (int k = 0; k < a.cnt; k++, pa += 128u) sum = sum + lds(pa);
                         const typename R::Ref r = rs.at(v);
                         if (!last) {
@@ -419,7 +428,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                             Row6 o = a.o;
                             R::st(r, S, sum);
                             set_k<S>(o, sum);
-                            sts(sb + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
+                            put_spin(v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
                         } else {
                             const Row6& o = a.o;
                             em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
@@ -460,12 +469,12 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                 const typename R::Ref r = rs.at(v);
                 Row6 o = load_row<S, R>(r);  // what the next stage's input (or stage 6) reads
                 float sum = 0.0f;
-#pragma unroll 4
+#pragma unroll 8
                 for (int k = r0; k < r1; k++, p += 128u) sum = sum + lds(p);
                 if constexpr (S < 6) {
                     R::st(r, S, sum);
                     set_k<S>(o, sum);
-                    sts(sb + 4u * (uint32_t)v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
+                    put_spin(v, row_input<S + 1>(o, S == 1 ? (float)hnext : hT));
                 } else {
                     em = fmaxf(em, rk_err_ratio(o.x, o.k1, o.k3, o.k4, o.k5, sum, hT, h0T, false));
                     R::st(r, 2, rk_new<float>(o.x, o.k1, o.k3, o.k4, sum, hT));
@@ -537,7 +546,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     const typename R::Ref r = rs.at(v);
                     const float xn = R::ld(r, 2);
                     R::st(r, 0, xn);
-                    sts(sb + 4u * (uint32_t)v, xn);
+                    put_spin(v, xn);
                 }
                 s1_ready = true;
             }
@@ -556,7 +565,10 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
 #pragma unroll
                     for (int q = 0; q < K; q++) {
                         const uint32_t w = ld_lit(lp + 32 * q);
-                        const uint32_t sa = ROWS_G ? sb + 4u * (w & 0x1FFFu) : (sb | (w & mask));
+                        // the positive spin (the word of a negated literal points at -s)
+                        const uint32_t sa = ROWS_G ? sb + 4u * (w & 0x1FFFu)
+                                                   : (w & 0x80000000u) ? (sb | (w & mask)) - 4u * (uint32_t)(n + 1)
+                                                                       : (sb | (w & mask));
                         const bool tv = lds(sa) > 0.0f;
                         sat |= (w & 0x80000000u) ? !tv : tv;
                     }
