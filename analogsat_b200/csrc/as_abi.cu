@@ -116,9 +116,8 @@ struct DevicePool {
                 for (int qq = 0; qq < q->k; qq++) {
                     const uint32_t w = q->lit[(size_t)qq * q->mp + c];
                     const uint32_t var = (w >> 16) & 0x7fffu, slot = w & 0xffffu;
-                    // a negated literal addresses the negated spin copy, which follows
-                    // the N + 1 spins (sentinel included)
-                    const uint32_t so = 4u * var + ((w & 0x80000000u) ? 4u * (uint32_t)(q->n + 1) : 0u);
+                    // a negated literal addresses the negated spin copy (neg_spin_base)
+                    const uint32_t so = 4u * var + ((w & 0x80000000u) ? 4u * (uint32_t)neg_spin_base(q->n) : 0u);
                     fw[f0 + lean_word_index(c, qq, q->k)] = (w & 0x80000000u) | (slot << 14) | so;
                 }
         }

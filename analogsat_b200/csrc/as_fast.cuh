@@ -44,15 +44,17 @@ namespace asb {
 // Shared-memory byte offsets of the lean layout for an instance, and whether its
 // literal words can carry them (spin offsets below 16 KB, slot indices below 2^17).
 // bytes: shared memory with the rows on chip; bytes_g: without them (ROWS_G).
-// The all-shared form holds the spins twice, s_0..s_N (s_N the sentinel) and then
-// -s_0..-s_N, so a negated literal's word points at its negated spin and a gather needs
-// no sign flip; both copies sit at a shared address aligned to spin_align (the smallest
-// power of two >= their bytes), so a spin's address is that base OR the byte offset of
-// its literal word: one logic operation.  bytes counts the worst-case padding.  The
-// global-rows form holds one copy; its slots start at cs_off_g.
+// The all-shared form holds the spins twice, s_0..s_N (s_N the sentinel) and, from the
+// next multiple of 32 floats (neg_spin_base, so -s_v sits in s_v's bank), -s_0..-s_N: a
+// negated literal's word points at its negated spin and a gather needs no sign flip.
+// Both copies sit at a shared address aligned to spin_align (the smallest power of two
+// >= their bytes), so a spin's address is that base OR the byte offset of its literal
+// word: one logic operation.  bytes counts the worst-case padding.  The global-rows
+// form holds one copy; its slots start at cs_off_g.
+__host__ __device__ inline int neg_spin_base(int n) { return (n + 1 + 31) & ~31; }
 __host__ __device__ inline uint32_t spin_align(int n) {
     uint32_t a = 128;
-    while (a < 8u * (uint32_t)(n + 1)) a <<= 1;
+    while (a < 4u * (uint32_t)(neg_spin_base(n) + n + 1)) a <<= 1;
     return a;
 }
 struct FastLayout {
@@ -62,12 +64,12 @@ struct FastLayout {
 };
 __host__ __device__ inline FastLayout fast_layout(int n, int m, int nslots) {
     FastLayout L;
-    L.cs_off = ((8 * (n + 1)) + 127) / 128 * 128;  // a multiple of 128 B keeps slot banks
+    L.cs_off = ((4 * (neg_spin_base(n) + n + 1)) + 127) / 128 * 128;  // a multiple of 128 B keeps slot banks
     L.cs_off_g = ((4 * (n + 1)) + 127) / 128 * 128;
     const long long cs_end = (long long)L.cs_off + 4ll * (nslots + 1);
     L.rows_off = (int)((cs_end + 15) / 16 * 16);
     L.bytes = (size_t)L.rows_off + 24ull * (size_t)(n + m) + spin_align(n) - 16;
-    L.ok = 8ll * (n + 1) <= 16384 && nslots < (1 << 17);
+    L.ok = 4ll * (neg_spin_base(n) + n + 1) <= 16384 && nslots < (1 << 17);
     return L;
 }
 
@@ -327,7 +329,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         else rs.base = sb + (uint32_t)I.rows_off;
         const uint32_t cs0 = sb + (uint32_t)cso;
         // the all-shared form's second, negated spin copy: spin v also at sneg + 4 v
-        const uint32_t sneg = sb + 4u * (uint32_t)(n + 1);
+        const uint32_t sneg = sb + 4u * (uint32_t)neg_spin_base(n);
         auto put_spin = [&](int v, float val) {
             sts(sb + 4u * (uint32_t)v, val);
             if constexpr (!ROWS_G) sts(sneg + 4u * (uint32_t)v, -val);
@@ -567,7 +569,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                         const uint32_t w = ld_lit(lp + 32 * q);
                         // the positive spin (the word of a negated literal points at -s)
                         const uint32_t sa = ROWS_G ? sb + 4u * (w & 0x1FFFu)
-                                                   : (w & 0x80000000u) ? (sb | (w & mask)) - 4u * (uint32_t)(n + 1)
+                                                   : (w & 0x80000000u) ? (sb | (w & mask)) - 4u * (uint32_t)neg_spin_base(n)
                                                                        : (sb | (w & mask));
                         const bool tv = lds(sa) > 0.0f;
                         sat |= (w & 0x80000000u) ? !tv : tv;
