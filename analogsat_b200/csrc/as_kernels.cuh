@@ -788,7 +788,7 @@ __global__ void __launch_bounds__(BT, 1) rhs_pair_kernel(DevInstance I, const fl
             const int r0 = (int)(vrows[i] & 0xffffu), r1 = (int)(vrows[i] >> 16);
             const float2* p = cs + r0 * 32 + (v & 31);
             float2 sum = f2(0.0f);
-#pragma unroll 4
+#pragma unroll 8
             for (int r = r0; r < r1; r++, p += 32) sum = __fadd2_rn(sum, *p);
             S0[vp[i]] = sum.x;
             S1[vp[i]] = sum.y;
