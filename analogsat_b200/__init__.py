@@ -170,13 +170,15 @@ class SatProblem:
 
 
 def _stream_ptr(stream):
+    """A CUDA stream handle: an int (cudaStream_t), an object with .cuda_stream (a
+    torch.cuda.Stream), or None for torch's current stream."""
     if stream is None:
         try:
             import torch
             return C.c_void_p(torch.cuda.current_stream().cuda_stream)
         except Exception:
             return C.c_void_p(0)
-    return C.c_void_p(int(stream))
+    return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
 
 
 def get_derivatives(problem: SatProblem, x, out=None, logspace: bool = False, stream=None):

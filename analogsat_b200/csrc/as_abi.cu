@@ -308,6 +308,17 @@ int preferred_bt(const PackedProblem& q) {
     return std::max(64, std::min(1024, bt));
 }
 
+// Raises a kernel's dynamic shared memory limit on the current device to at least
+// `bytes`; never lowers it, so a limit that another launch group or solver (whose
+// launches may sit in a captured graph) relies on stays in place.
+cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, fn);
+    if (e != cudaSuccess) return e;
+    if ((size_t)a.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // CTA size of a shared-memory launch: a trajectory of `smem_bytes` that leaves no room
 // for a second CTA on its SM gets the largest CTA (more warps to hide the clause
 // phase's latencies), smaller ones `bt`.
@@ -1021,7 +1032,7 @@ int build_groups(as_solver* s) {
         }
         G.bt = s->forced_bt ? s->forced_bt : (v.gs && !v.lean ? (v.cl > 1 ? 1024 : gs_bt) : sm_bt);
         G.smem = sbytes;
-        AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem));
+        AS_CUDA(raise_smem_limit((const void*)v.fn, G.smem));
         int occ = 0;
         if (v.cl > 1) {
             AS_CUDA(cudaFuncSetAttribute(v.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -1913,7 +1924,7 @@ int32_t as_solver_solve_noalloc(as_solver* s, int32_t problem_index, int32_t num
         s->wall_budget > 0.0 ? (unsigned long long)(s->wall_budget * 1e9) : 0ull);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("prepare launch: ") + cudaGetErrorString(e));
-    e = cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = raise_smem_limit((const void*)v->fn, smem);
     if (e != cudaSuccess) return fail(AS_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     int occ = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v->fn, bt, smem);

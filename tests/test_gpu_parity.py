@@ -416,3 +416,43 @@ def test_lean_kernel_global_rows_matches_generic_kernel(n, m):
         assert np.array_equal(ra[key], rb[key]), key
     np.testing.assert_allclose(xb, xa, rtol=1e-6, atol=1e-6)
     print(n, "bit-identical" if np.array_equal(xa, xb) else f"max diff {np.abs(xa - xb).max():.3g}")
+
+
+def test_solvers_of_different_sizes_interleave(golden):
+    """Two solvers that launch the same kernel with different shared-memory footprints:
+    the large one solves, a small one solves, then the large one solves again -- once
+    re-recorded (a setter drops its captured solve) and once launched directly on a
+    caller's stream.  A kernel's shared-memory limit is a per-device setting, so the
+    small solver must not lower it below what the large one's launches need; both
+    repeats give the first run's results."""
+    import torch
+    from analogsat_b200 import AS_PREC_F32_LOGA
+    from analogsat_b200.instances import initial_states
+
+    def make(tag, seed):
+        n, m, _ = (int(v) for v in golden[f"{tag}/nmk"])
+        s = _solver(golden, tag, AS_PREC_F32_LOGA, 1e-6, 25, 200)
+        s.SetSatStates(np.zeros(4, np.int32), initial_states(n, m, 4, seed=seed, dtype=np.float32))
+        return s
+
+    big = make("p1000", 91)
+    big.Solve()
+    first = (big.results(), big.GetSatStates(np.float32))
+    small = make("p50", 92)
+    small.Solve()
+    assert big.launch_shape()["smem_bytes"] > small.launch_shape()["smem_bytes"]
+    assert big.kernel_name() == small.kernel_name() == "solve_kernel_fast"
+    ics = initial_states(*(int(v) for v in golden["p1000/nmk"][:2]), 4, seed=91, dtype=np.float32)
+    for direct in (False, True):
+        big.SetMaxSteps(200)  # drops the captured solve
+        big.SetSatStates(np.zeros(4, np.int32), ics)
+        if direct:
+            st = torch.cuda.Stream()
+            big.SolveAsync(st.cuda_stream)
+            big.Sync()
+        else:
+            big.Solve()
+        again = (big.results(), big.GetSatStates(np.float32))
+        for key in ("status", "steps", "rhs"):
+            assert np.array_equal(first[0][key], again[0][key]), (direct, key)
+        assert np.array_equal(first[1], again[1]), direct
