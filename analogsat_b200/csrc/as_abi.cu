@@ -639,7 +639,7 @@ int launch_per_state(as_problem* p, int prec, void (*fs)(DevInstance, const T*, 
     AS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     const size_t smem = vals * sizeof(T);
     if (compact && smem + 1024 <= (size_t)optin) {
-        AS_CUDA(cudaFuncSetAttribute(fs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        AS_CUDA(raise_smem_limit((const void*)fs, smem));
         AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fs, bt, smem));
         const int grid = std::max(1, std::min(ns, sms * std::max(occ, 1)));
         fs<<<grid, bt, smem, st>>>(p->dev[prec].host_inst[0], x, out, ns, stride, (T*)nullptr, 0ll);
@@ -674,7 +674,7 @@ int launch_rhs_pair(as_problem* p, const float* x, float* d, int ns, cudaStream_
     int r = ensure_uploaded(p, kLayoutPair);
     if (r) return r;
     auto fn = &rhs_pair_kernel<LOGA, KMAX, EXACT, BT, CPT, VPT>;
-    AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    AS_CUDA(raise_smem_limit((const void*)fn, smem));
     AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BT, smem));
     if (occ < 1) return AS_OK;
     const int grid = std::max(1, std::min((ns + 1) / 2, sms * occ));
@@ -2065,7 +2065,7 @@ int32_t as_solver_adjoint(as_solver* s, double t_end, int32_t max_steps, const d
     P.t_end = t_end;
 
     auto launch = [&](AdjFn fn) -> int {
-        AS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        AS_CUDA(raise_smem_limit((const void*)fn, smem));
         int occ = 0;
         AS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, bt, smem));
         if (occ < 1) return fail(AS_ERR_UNSUPPORTED, "adjoint launch shape does not fit on an SM");
