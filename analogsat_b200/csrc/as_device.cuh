@@ -150,6 +150,11 @@ template <typename T, bool LOGA, int KMAX, bool EXACT, int ENC>
 __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* __restrict__ sy,
                                           T* __restrict__ cs, T am, T knorm) {
     using A = Arith<T>;
+    // FP32 with log-space weights folds the power-of-two scalings (knorm = 2^-k): km
+    // holds P = f_0 .. f_{k-1} (K_m = knorm P), and 2 r = P (a_m 2 knorm^2), du_m =
+    // (P P)(knorm^2 / ln 2) -- the same roundings as the unfolded forms, since a
+    // power-of-two factor scales a rounded product exactly (the lean kernel forms them so)
+    constexpr bool kFold = LOGA && sizeof(T) == 4;
     Lit<ENC> w[KMAX];
     T f[KMAX];
     T km = knorm;
@@ -162,11 +167,12 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
                 f[q] = T(1) - __int_as_float(__float_as_int(s) ^ (int)(w[q].w & 0x80000000u));
             else
                 f[q] = w[q].neg() ? A::add(T(1), s) : A::sub(T(1), s);
-            km = A::mul(km, f[q]);
+            km = (kFold && q == 0) ? f[q] : A::mul(km, f[q]);
         }
     }
     T dam;
-    if constexpr (LOGA) dam = km * km * T(kInvLn2);
+    if constexpr (kFold) dam = (km * km) * (knorm * knorm * T(kInvLn2));
+    else if constexpr (LOGA) dam = km * km * T(kInvLn2);
     else dam = A::mul(A::mul(am, km), km);
     if (I.tanh) {
         // CpuSatTanh: knorm a_m |K_mi| tanh(q (1 - c s_i)) c_mi (KmiFuncTanh,
@@ -208,7 +214,8 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
         return dam;
     }
     if (KMAX <= 10 || I.k <= 10) {
-        const T r = A::mul(A::mul(km, knorm), am);
+        // r (r2 = 2 r when folded)
+        const T r = kFold ? km * (am * (T(2) * knorm * knorm)) : A::mul(A::mul(km, knorm), am);
 #pragma unroll
         for (int q = 0; q < KMAX; q++) {
             if (EXACT || q < I.k) {
@@ -222,7 +229,7 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
                     }
                 }
                 if constexpr (sizeof(T) == 4) {  // (2r) prod == 2 (r prod) above the subnormals
-                    const T rr = (r + r) * prod;
+                    const T rr = (kFold ? r : r + r) * prod;
                     cs[w[q].slot()] = __int_as_float(__float_as_int(rr) ^ (int)(w[q].w & 0x80000000u));
                 } else {
                     T rr = A::mul(r, prod);
@@ -235,7 +242,7 @@ __device__ __forceinline__ T clause_phase(const DevInstance& I, int m, const T* 
 #pragma unroll
         for (int q = 0; q < KMAX; q++) {
             if (EXACT || q < I.k) {
-                T temp = km;
+                T temp = kFold ? knorm * km : km;
 #pragma unroll
                 for (int l = 0; l < KMAX; l++)
                     if (EXACT || l < I.k) temp = A::mul(temp, l == q ? T(1) : f[l]);

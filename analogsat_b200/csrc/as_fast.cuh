@@ -196,21 +196,25 @@ __device__ __forceinline__ float lit_factor(uint32_t sb, uint32_t mask, uint32_t
 
 // Clause phase of one clause (K literals, FP32, log-space weights): spin gathers,
 // K_m, the leave-one-out products in CpuProdWrapper order, contributions into their
-// slots; returns du_m = K_m^2 / ln 2.  Same operations as clause_phase<float, true, K>.
+// slots; returns du_m = K_m^2 / ln 2.  Same operations as clause_phase<float, true, K>,
+// with its power-of-two scalings folded: with P = f_0 f_1 .. f_{K-1}, K_m = knorm P and
+// 2 r = 2 (K_m knorm) a_m = P (a_m 2 knorm^2), du_m = (P P)(knorm^2 / ln 2) -- the same
+// roundings (a power-of-two factor scales a rounded product exactly).  am2 = a_m 2
+// knorm^2, duc = knorm^2 / ln 2.
 template <int K>
-__device__ __forceinline__ float fast_clause(uint32_t sb, uint32_t mask, uint32_t cs0, const uint32_t* lp, float am,
-                                             float knorm) {
+__device__ __forceinline__ float fast_clause(uint32_t sb, uint32_t mask, uint32_t cs0, const uint32_t* lp, float am2,
+                                             float duc) {
     uint32_t w[K];
     float f[K];
 #pragma unroll
     for (int q = 0; q < K; q++) w[q] = ld_lit(lp + 32 * q);
-    float km = knorm;
+    float P = 0.0f;
 #pragma unroll
     for (int q = 0; q < K; q++) {
         f[q] = lit_factor(sb, mask, w[q]);
-        km = km * f[q];
+        P = q == 0 ? f[0] : P * f[q];
     }
-    const float r = (km * knorm) * am;
+    const float r2 = P * am2;
 #pragma unroll
     for (int q = 0; q < K; q++) {
         float prod = 1.0f;
@@ -222,28 +226,28 @@ __device__ __forceinline__ float fast_clause(uint32_t sb, uint32_t mask, uint32_
                 first = false;
             }
         }
-        const float rr = (r + r) * prod;  // (2r) prod == 2 (r prod) above the subnormals
+        const float rr = r2 * prod;  // (2r) prod == 2 (r prod) above the subnormals
         sts(cs0 + 4u * ((w[q] >> 14) & 0x1FFFFu), __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u)));
     }
-    return km * km * kInvLn2;
+    return (P * P) * duc;
 }
 
 // The same on a clause-parts word (bits 0-12 internal variable, 13-29 slot, 31 sign).
 template <int K>
-__device__ __forceinline__ float part_clause(uint32_t sm0, uint32_t cs0, const uint32_t* lp, float am,
-                                             float knorm) {
+__device__ __forceinline__ float part_clause(uint32_t sm0, uint32_t cs0, const uint32_t* lp, float am2,
+                                             float duc) {
     uint32_t w[K];
     float f[K];
 #pragma unroll
     for (int q = 0; q < K; q++) w[q] = ld_lit(lp + 32 * q);
-    float km = knorm;
+    float P = 0.0f;
 #pragma unroll
     for (int q = 0; q < K; q++) {
         const float sv = lds(sm0 + 4u * (w[q] & 0x1FFFu));
         f[q] = 1.0f - __int_as_float(__float_as_int(sv) ^ (int)(w[q] & 0x80000000u));
-        km = km * f[q];
+        P = q == 0 ? f[0] : P * f[q];
     }
-    const float r = (km * knorm) * am;
+    const float r2 = P * am2;
 #pragma unroll
     for (int q = 0; q < K; q++) {
         float prod = 1.0f;
@@ -255,10 +259,10 @@ __device__ __forceinline__ float part_clause(uint32_t sm0, uint32_t cs0, const u
                 first = false;
             }
         }
-        const float rr = (r + r) * prod;
+        const float rr = r2 * prod;
         sts(cs0 + 4u * ((w[q] >> 13) & 0x1FFFFu), __int_as_float(__float_as_int(rr) ^ (int)(w[q] & 0x80000000u)));
     }
-    return km * km * kInvLn2;
+    return (P * P) * duc;
 }
 
 // Block max of the error ratios, post-processed by thread 0.  The ratios are FP32 and
@@ -336,6 +340,8 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
         };
         float* G = reinterpret_cast<float*>(P.states) + P.unit_state[u];
         const float knorm = (float)ldexp(1.0, -I.k);
+        const float a2n = 2.0f * knorm * knorm;      // 2 knorm^2 (exact)
+        const float duc = knorm * knorm * kInvLn2;   // knorm^2 / ln 2 (exact scaling)
         // the wall-clock deadline (stamped before the launch)
         const unsigned long long deadline = P.deadline ? *P.deadline : 0ull;
 
@@ -383,7 +389,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
                     typename R::Ref ra = rs.at(cb + c0 + tid);
                     for (int c = c0 + tid; c < c1; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                         const Row6 o = load_clause_row<S, R>(ra, ready);
-                        const float d = part_clause<K>(sb, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+                        const float d = part_clause<K>(sb, cs0, lp, exp2_fast(row_input<S>(o, hT)) * a2n, duc);
                         if constexpr (S < 6) {
                             R::st(ra, S, d);
                         } else {
@@ -453,7 +459,7 @@ __global__ void __launch_bounds__(1024, 1) solve_kernel_fast(SolveParams P) {
             typename R::Ref ra = rs.at(cb + tid);
             for (int c = tid; c < m; c += nt, lp += (size_t)nt * K, ra = R::advance(ra, nt)) {
                 const Row6 o = load_clause_row<S, R>(ra, ready);
-                const float d = fast_clause<K>(sb, mask, cs0, lp, exp2_fast(row_input<S>(o, hT)), knorm);
+                const float d = fast_clause<K>(sb, mask, cs0, lp, exp2_fast(row_input<S>(o, hT)) * a2n, duc);
                 if constexpr (S < 6) {
                     R::st(ra, S, d);
                 } else {
