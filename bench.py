@@ -473,14 +473,14 @@ def run_ours(args):
         "clocks": clocks,
     }
     if line["roofline"]["kernel"] == "solve_kernel_fast" and W["n"] == 1000:
-        # the kernel's actual limit is instruction issue: ncu counts 11.97k warp-instructions
+        # the kernel's actual limit is instruction issue: ncu counts 11.5k warp-instructions
         # per RHS for it on this instance size; the peak is 4 warp-instructions per cycle
         # on each SM at the SM clock sampled during the timed region
         sm_hz = float(clocks.get("sm_mhz") or 1965.0) * 1e6
-        wi = 11.97e3 * (totals["rhs"] / kern_s)
+        wi = 11.5e3 * (totals["rhs"] / kern_s)
         import torch
         peak_wi = 4 * sm_hz * torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-        line["roofline"]["issue"] = {"warp_instructions_per_rhs": 11.97e3, "achieved": wi / 1e9,
+        line["roofline"]["issue"] = {"warp_instructions_per_rhs": 11.5e3, "achieved": wi / 1e9,
                                      "peak": peak_wi / 1e9, "unit": "G warp-instructions/s",
                                      "frac": wi / peak_wi}
     line.update(extras)
