@@ -4,15 +4,22 @@
 // + CpuRungeKutta::Step/rkqs/rkck + CpuSat::GetDerivatives/GetClauseViolationCount:
 // AnalogSAT/solver/SatSolver.h:273-355, AnalogSAT/cpu_sat/CpuRungeKutta.cpp:66-100,
 // 181-267, AnalogSAT/cpu_sat/CpuSat.cpp:65-94,136-173,199-241) and the same FP32
-// arithmetic in the same expression order, with the instruction count per clause cut
-// down -- the shared-memory solver is issue bound, so its RHS rate is the inverse of
-// the instructions it executes per clause and stage:
+// arithmetic as its log-space FP32 path (bit-identical results), with the instruction
+// count per clause cut down -- the shared-memory solver is issue bound, so its RHS rate
+// is the inverse of the instructions it executes per clause and stage:
 //
 //  * Literal words carry shared-memory addressing (DevInstance::flit): bits 0-13 the
 //    byte offset of the literal's spin from the spin base (aligned to a power of two
 //    at least the spins' size, so base | offset is the address), bits 14-30 the index
-//    of its contribution slot, bit 31 the sign.  A spin gather is one logic operation
-//    and one load, a contribution store a shift, a mask, a scaled add and a store.
+//    of its contribution slot, bit 31 the sign.  The spins are held twice, the second
+//    copy negated (neg_spin_base), and a negated literal's word points into it: a spin
+//    gather is one logic operation and one load, with no sign flip.
+//  * The clause arithmetic folds its power-of-two scalings (fast_clause), as the
+//    general kernel's FP32 log-space path does.
+//  * Each stage's variable phase also forms the next stage's spin input, and an
+//    accepted step's copy of the clause rows happens in the next stage 1's clause
+//    loop; the error max is an integer redux (lean_max_then) and an accepted step's
+//    next step size is formed in the next stage 1 (settle_h).
 //  * Literal words are blocked by 32 clauses ([m / 32][q][m % 32]), so a clause's K
 //    words are loads at immediate offsets from one pointer that advances once per
 //    clause, and a warp's 32 clauses load each word as one 128-byte line.
@@ -43,7 +50,8 @@ namespace asb {
 
 // Shared-memory byte offsets of the lean layout for an instance, and whether its
 // literal words can carry them (spin offsets below 16 KB, slot indices below 2^17).
-// bytes: shared memory with the rows on chip; bytes_g: without them (ROWS_G).
+// bytes: shared memory of the all-shared form (rows on chip); cs_off_g: where the
+// global-rows form's slots start (one spin copy).
 // The all-shared form holds the spins twice, s_0..s_N (s_N the sentinel) and, from the
 // next multiple of 32 floats (neg_spin_base, so -s_v sits in s_v's bank), -s_0..-s_N: a
 // negated literal's word points at its negated spin and a gather needs no sign flip.
