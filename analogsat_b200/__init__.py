@@ -293,7 +293,8 @@ class SatSolver:
     # -- states (SatSolver::SetSatState, SatSolver.h:183-192) --
     def SetSatStates(self, problem_index, states, stream=None):
         """states: host array of the concatenated public vectors, or a CUDA tensor
-        (copied device-to-device on `stream`, default the current torch stream)."""
+        (copied device-to-device on `stream` -- a cudaStream_t handle or a
+        torch.cuda.Stream -- default the current torch stream)."""
         pi = _i32(problem_index)
         self._traj_problem = pi.copy()
         try:
@@ -341,6 +342,9 @@ class SatSolver:
         return self.results()["status"]
 
     def SolveAsync(self, stream=None):
+        """Enqueue the solve without waiting (as_solver_solve_async): on the solver's own
+        stream, or on `stream` (a cudaStream_t handle or a torch.cuda.Stream), ordered
+        after the states set before and before the reads queued after; Sync() waits."""
         check(self._lib.as_solver_solve_async(self._h, _stream_ptr(stream) if stream else None))
 
     def Sync(self):
