@@ -152,3 +152,16 @@ def test_result_messages():
             4: b"maximum steps reached", 5: b"unknown result", 99: b"unknown result"}
     for code, msg in msgs.items():
         assert lib.as_result_message(code) == msg
+
+
+def test_stream_arguments_accept_handles_and_stream_objects():
+    """Stream arguments of the Python API take a raw cudaStream_t handle or any object
+    with a .cuda_stream handle (a torch.cuda.Stream); both reach the C ABI as the same
+    pointer value."""
+    from analogsat_b200 import _stream_ptr
+
+    class FakeStream:
+        cuda_stream = 0x1234
+
+    assert _stream_ptr(0x1234).value == 0x1234
+    assert _stream_ptr(FakeStream()).value == 0x1234
